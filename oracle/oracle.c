@@ -1,0 +1,555 @@
+/*
+ * oracle.c -- FP64 CPU restatement of sma-dft's time-step loop (TEST INFRASTRUCTURE ONLY).
+ * See oracle.h.  Every block cites the reference lines it restates; the operation order
+ * follows the reference so that FP64 results agree to rounding.
+ */
+#include "oracle.h"
+#include "r2r.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define T10 ORC_REDFT10
+#define T01 ORC_REDFT01
+#define S10 ORC_RODFT10
+#define S01 ORC_RODFT01
+
+struct orc_ctx {
+    orc_params p;
+    int nx, ny, nz;
+    long n;
+    double Lx, Ly, Lz, dx, dy, dz, scale;
+    double rho_m, lambda;
+    /* DCT wavenumbers q_i = pi i / L and DST wavenumbers s_i = pi (i+1) / L */
+    double *qx, *qy, *qz, *sx, *sy, *sz;
+    double *aLin, *C1, *C2, *mq2;
+    double *CM1x, *CM1y, *CM1z, *CM2x, *CM2y, *CM2z;
+    double *psi, *psiq, *psiNew, *Nr, *Nq, *NqPast;
+    /* advection */
+    double *gx, *gy, *gz, *sp2, *Sx, *Sy, *Sz, *vx, *vy, *vz;
+    /* quasi */
+    double *psiq_old, *psi_old, *rho, *rhoq, *rho_old, *p_, *divv, *mu, *energy, *dfd, *lap;
+    double *rdx, *rdy, *rdz;
+    long nloop;
+    double L1, mass, en;
+    int have_psi;
+};
+
+#define IDX(c, i, j, k) (((long)(i) * (c)->ny + (j)) * (c)->nz + (k))
+
+static double *dal(long n) { return (double *)calloc((size_t)n, sizeof(double)); }
+
+void orc_r2r_3d_kinds(const double *in, double *out, int nx, int ny, int nz, int kx, int ky, int kz)
+{
+    orc_r2r_3d(in, out, nx, ny, nz, kx, ky, kz);
+}
+
+static void r3(orc_ctx *c, const double *in, double *out, int kx, int ky, int kz)
+{
+    orc_r2r_3d(in, out, c->nx, c->ny, c->nz, kx, ky, kz);
+}
+
+orc_ctx *orc_create(const orc_params *p)
+{
+    if (p->nx < 2 || p->ny < 2 || p->nz < 2) return NULL;
+    orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
+    c->p = *p;
+    c->nx = p->nx; c->ny = p->ny; c->nz = p->nz;
+    c->n = (long)c->nx * c->ny * c->nz;
+    /* box and grid: no-adv/cosNoAdvTrackSing.cpp:160-172 */
+    c->Lx = c->nx * 2.0 * M_PI / (p->q0 * p->nw);
+    c->Ly = c->ny * 2.0 * M_PI / (p->q0 * p->nw);
+    c->Lz = c->nz * 2.0 * M_PI / (p->q0 * p->nw);
+    c->dx = c->Lx / c->nx; c->dy = c->Ly / c->ny; c->dz = c->Lz / c->nz;
+    c->scale = 0.125 / ((double)c->nx * c->ny * c->nz);
+    /* quasi constants: quasi/quasi.cpp:237-246 */
+    double rho_s = p->kp * p->amp + p->rho0;
+    c->rho_m = rho_s / 2;
+    c->lambda = -2 * p->nu / 3;
+    /* wavenumbers: no-adv/cosNoAdvTrackSing.cpp:309-324 (DCT), adv/cosAdvTrackMult.cpp:386-401 (DST) */
+    c->qx = dal(c->nx); c->sx = dal(c->nx);
+    c->qy = dal(c->ny); c->sy = dal(c->ny);
+    c->qz = dal(c->nz); c->sz = dal(c->nz);
+    for (int i = 0; i < c->nx; i++) { c->qx[i] = 1.0 * M_PI * i / (c->dx * c->nx); c->sx[i] = 1.0 * M_PI * (i + 1) / (c->dx * c->nx); }
+    for (int j = 0; j < c->ny; j++) { c->qy[j] = M_PI * (j) / (c->dy * c->ny); c->sy[j] = M_PI * (j + 1) / (c->dy * c->ny); }
+    for (int k = 0; k < c->nz; k++) { c->qz[k] = M_PI * (k) / (c->dz * c->nz); c->sz[k] = M_PI * (k + 1) / (c->dz * c->nz); }
+    long n = c->n;
+    c->aLin = dal(n); c->C1 = dal(n); c->C2 = dal(n); c->mq2 = dal(n);
+    c->psi = dal(n); c->psiq = dal(n); c->psiNew = dal(n); c->Nr = dal(n); c->Nq = dal(n); c->NqPast = dal(n);
+    if (p->model != ORC_NOADV) {
+        c->CM1x = dal(n); c->CM1y = dal(n); c->CM1z = dal(n);
+        c->CM2x = dal(n); c->CM2y = dal(n); c->CM2z = dal(n);
+        c->gx = dal(n); c->gy = dal(n); c->gz = dal(n); c->sp2 = dal(n);
+        c->Sx = dal(n); c->Sy = dal(n); c->Sz = dal(n);
+        c->vx = dal(n); c->vy = dal(n); c->vz = dal(n);
+    }
+    if (p->model == ORC_QUASI) {
+        c->psiq_old = dal(n); c->psi_old = dal(n); c->rho = dal(n); c->rhoq = dal(n);
+        c->rho_old = dal(n); c->p_ = dal(n); c->divv = dal(n); c->mu = dal(n); c->energy = dal(n);
+        c->dfd = dal(n); c->lap = dal(n); c->rdx = dal(n); c->rdy = dal(n); c->rdz = dal(n);
+    }
+    /* linear operator and Stokes coefficients:
+     * noadv  no-adv/cosNoAdvTrackSing.cpp:594-602
+     * adv    adv/cosAdvTrackMult.cpp:729-751
+     * quasi  quasi/quasi.cpp:963-985 (C1 = 2 - dt rho_m L, C2 = 1.5 - dt rho_m L) */
+    const double dtd2 = p->dt / 2;
+    for (int i = 0; i < c->nx; i++)
+        for (int j = 0; j < c->ny; j++)
+            for (int k = 0; k < c->nz; k++) {
+                long idx = IDX(c, i, j, k);
+                double mq2 = pow(c->qx[i], 2) + pow(c->qy[j], 2) + pow(c->qz[k], 2);
+                c->mq2[idx] = mq2;
+                double q02 = p->q0 * p->q0;
+                if (p->model == ORC_QUASI) {
+                    double opSH = p->alpha * pow(q02 - mq2, 2);
+                    c->aLin[idx] = p->eps - opSH;
+                    c->C1[idx] = (2.0 - p->dt * c->rho_m * c->aLin[idx]);
+                    c->C2[idx] = (1.5 - p->dt * c->rho_m * c->aLin[idx]);
+                } else {
+                    double opSH = p->alpha * pow(mq2 - q02, 2);
+                    c->aLin[idx] = p->eps - opSH;
+                    c->C1[idx] = (1.0 + dtd2 * c->aLin[idx]);
+                    c->C2[idx] = (1.0 - dtd2 * c->aLin[idx]);
+                }
+                if (p->model != ORC_NOADV) {
+                    double m2 = pow(c->sx[i], 2) + pow(c->qy[j], 2) + pow(c->qz[k], 2);
+                    c->CM1x[idx] = c->scale / (p->nu * m2);
+                    c->CM2x[idx] = c->sx[i] / m2;
+                    m2 = pow(c->qx[i], 2) + pow(c->sy[j], 2) + pow(c->qz[k], 2);
+                    c->CM1y[idx] = c->scale / (p->nu * m2);
+                    c->CM2y[idx] = c->sy[j] / m2;
+                    m2 = pow(c->qx[i], 2) + pow(c->qy[j], 2) + pow(c->sz[k], 2);
+                    c->CM1z[idx] = c->scale / (p->nu * m2);
+                    c->CM2z[idx] = c->sz[k] / m2;
+                }
+            }
+    return c;
+}
+
+void orc_destroy(orc_ctx *c)
+{
+    if (!c) return;
+    double **ptrs[] = {&c->qx, &c->qy, &c->qz, &c->sx, &c->sy, &c->sz, &c->aLin, &c->C1, &c->C2,
+                       &c->mq2, &c->CM1x, &c->CM1y, &c->CM1z, &c->CM2x, &c->CM2y, &c->CM2z,
+                       &c->psi, &c->psiq, &c->psiNew, &c->Nr, &c->Nq, &c->NqPast, &c->gx, &c->gy,
+                       &c->gz, &c->sp2, &c->Sx, &c->Sy, &c->Sz, &c->vx, &c->vy, &c->vz,
+                       &c->psiq_old, &c->psi_old, &c->rho, &c->rhoq, &c->rho_old, &c->p_,
+                       &c->divv, &c->mu, &c->energy, &c->dfd, &c->lap, &c->rdx, &c->rdy, &c->rdz};
+    for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); q++) free(*ptrs[q]);
+    free(c);
+}
+
+/* N = beta psi^3 - gamma psi^5, no-adv/cosNoAdvTrackSing.cpp:713-723 */
+static void nonlin(orc_ctx *c, const double *psi, double *out)
+{
+    const double b = c->p.beta, g = c->p.gamma;
+    for (long q = 0; q < c->n; q++) out[q] = b * pow(psi[q], 3) - g * pow(psi[q], 5);
+}
+
+int orc_set_psi(orc_ctx *c, const double *psi0)
+{
+    long n = c->n;
+    memcpy(c->psi, psi0, sizeof(double) * n);
+    c->nloop = 0;
+    c->L1 = c->mass = c->en = 0.0;
+    if (c->p.model == ORC_QUASI) {
+        /* quasi/quasi.cpp:990-1034: psiq = scale CT(psi), psi = iCT(psiq), N^0, psiq_old, psi_old */
+        r3(c, c->psi, c->psiq, T10, T10, T10);
+        for (long q = 0; q < n; q++) c->psiq[q] = c->scale * c->psiq[q];
+        r3(c, c->psiq, c->psi, T01, T01, T01);
+        nonlin(c, c->psi, c->Nr);
+        memcpy(c->psiq_old, c->psiq, sizeof(double) * n);
+        r3(c, c->Nr, c->Nq, T10, T10, T10);
+        memcpy(c->psi_old, c->psi, sizeof(double) * n);
+        memset(c->divv, 0, sizeof(double) * n);
+        memset(c->rhoq, 0, sizeof(double) * n);
+        memset(c->rho_old, 0, sizeof(double) * n);
+        memset(c->vx, 0, sizeof(double) * n);
+        memset(c->vy, 0, sizeof(double) * n);
+        memset(c->vz, 0, sizeof(double) * n);
+    } else {
+        /* pre-loop N^0 (no advection term): no-adv/cosNoAdvTrackSing.cpp:618-635,
+         * adv/cosAdvTrackMult.cpp:760-777.  The wall potential has sigma = 0 (:75-82). */
+        nonlin(c, c->psi, c->Nr);
+        r3(c, c->Nr, c->Nq, T10, T10, T10);
+        if (c->p.model == ORC_NOADV) {
+            /* psiq is recomputed every step; keep the scaled transform for orc_get */
+            r3(c, c->psi, c->psiq, T10, T10, T10);
+            for (long q = 0; q < n; q++) c->psiq[q] *= c->scale;
+        } else {
+            r3(c, c->psi, c->psiq, T10, T10, T10);
+            for (long q = 0; q < n; q++) c->psiq[q] *= c->scale;
+        }
+    }
+    c->have_psi = 1;
+    return 0;
+}
+
+/* L1 = sum|new - old| / (dt sum|new|): no-adv/cosNoAdvTrackSing.cpp:775-789 */
+static double l1_measure(const orc_ctx *c, const double *newv, const double *oldv)
+{
+    double a = 0.0, b = 0.0;
+    for (long q = 0; q < c->n; q++) {
+        a = a + fabs(newv[q] - oldv[q]);
+        b = b + fabs(newv[q]);
+    }
+    return a / (c->p.dt * b);
+}
+
+/* ---------------- noadv: no-adv/cosNoAdvTrackSing.cpp:681-764,1072 ---------------- */
+static void step_noadv(orc_ctx *c)
+{
+    const long n = c->n;
+    const double dtd2 = c->p.dt / 2;
+    memcpy(c->NqPast, c->Nq, sizeof(double) * n);                 /* :688 */
+    nonlin(c, c->psi, c->Nr);                                      /* :713-723 */
+    r3(c, c->Nr, c->Nq, T10, T10, T10);                            /* :727 */
+    r3(c, c->psi, c->psiq, T10, T10, T10);                         /* :731 */
+    for (long q = 0; q < n; q++)                                   /* :752-753 */
+        c->psiq[q] = c->scale * (c->C1[q] * c->psiq[q] + dtd2 * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
+    r3(c, c->psiq, c->psiNew, T01, T01, T01);                      /* :758 */
+    c->L1 = l1_measure(c, c->psiNew, c->psi);                      /* :769-789 */
+    memcpy(c->psi, c->psiNew, sizeof(double) * n);                 /* :1072 */
+}
+
+/* Stokes velocity from the force spectra (adv/cosAdvTrackMult.cpp:1103-1274 on one rank;
+ * quasi adds the irrotational part, quasi/quasi.cpp:1704-2109).  Truncations: v_x at
+ * i = nx-1 is 0; v_y, v_z at j = ny-1 or k = nz-1 are 0; the shifted neighbours at
+ * index -1 are 0 (the single-rank halo planes stay zero-filled, adv :1157, quasi :1841). */
+static void stokes(orc_ctx *c, int with_divv)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const double nu = c->p.nu;
+    memset(c->vx, 0, sizeof(double) * c->n);
+    memset(c->vy, 0, sizeof(double) * c->n);
+    memset(c->vz, 0, sizeof(double) * c->n);
+    for (int i = 0; i < nx - 1; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                long idx = IDX(c, i, j, k);
+                double Sy = (j != 0) ? c->Sy[IDX(c, i + 1, j - 1, k)] : 0.0;
+                double Sz = (k != 0) ? c->Sz[IDX(c, i + 1, j, k - 1)] : 0.0;
+                double dot = c->sx[i] * c->Sx[idx] + c->qy[j] * Sy + c->qz[k] * Sz;
+                double v = c->CM1x[idx] * (c->Sx[idx] - c->CM2x[idx] * dot);
+                if (with_divv) v = v + c->CM1x[idx] * (nu * c->sx[i] * c->divv[IDX(c, i + 1, j, k)]);
+                c->vx[idx] = v;
+            }
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny - 1; j++)
+            for (int k = 0; k < nz - 1; k++) {
+                long idx = IDX(c, i, j, k);
+                double Sx = (i != 0) ? c->Sx[IDX(c, i - 1, j + 1, k)] : 0.0;
+                double Sz = (k != 0) ? c->Sz[IDX(c, i, j + 1, k - 1)] : 0.0;
+                double dot = c->qx[i] * Sx + c->sy[j] * c->Sy[idx] + c->qz[k] * Sz;
+                double v = c->CM1y[idx] * (c->Sy[idx] - c->CM2y[idx] * dot);
+                if (with_divv) v = v + c->CM1y[idx] * (nu * c->sy[j] * c->divv[IDX(c, i, j + 1, k)]);
+                c->vy[idx] = v;
+
+                Sx = (i != 0) ? c->Sx[IDX(c, i - 1, j, k + 1)] : 0.0;
+                double Sy = (j != 0) ? c->Sy[IDX(c, i, j - 1, k + 1)] : 0.0;
+                dot = c->qx[i] * Sx + c->qy[j] * Sy + c->sz[k] * c->Sz[idx];
+                v = c->CM1z[idx] * (c->Sz[idx] - c->CM2z[idx] * dot);
+                if (with_divv) v = v + c->CM1z[idx] * (nu * c->sz[k] * c->divv[IDX(c, i, j, k + 1)]);
+                c->vz[idx] = v;
+            }
+}
+
+/* Gradient spectra by index shift (adv/cosAdvTrackMult.cpp:904-959): G_x[i] = -s_i f[i+1],
+ * last index along the shifted axis left 0. */
+static void shift_grad(orc_ctx *c, const double *f, double *gxo, double *gyo, double *gzo)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    memset(gxo, 0, sizeof(double) * c->n);
+    memset(gyo, 0, sizeof(double) * c->n);
+    memset(gzo, 0, sizeof(double) * c->n);
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                long idx = IDX(c, i, j, k);
+                if (i < nx - 1) gxo[idx] = -c->sx[i] * f[IDX(c, i + 1, j, k)];
+                if (j < ny - 1) gyo[idx] = -c->sy[j] * f[IDX(c, i, j + 1, k)];
+                if (k < nz - 1) gzo[idx] = -c->sz[k] * f[IDX(c, i, j, k + 1)];
+            }
+}
+
+/* ---------------- adv: adv/cosAdvTrackMult.cpp:824-1369,1742 ---------------- */
+static void step_adv(orc_ctx *c)
+{
+    const long n = c->n;
+    const double dtd2 = c->p.dt / 2, b = c->p.beta, g = c->p.gamma;
+    memcpy(c->NqPast, c->Nq, sizeof(double) * n);                  /* :842 */
+    r3(c, c->psi, c->psiq, T10, T10, T10);                          /* :847 */
+    for (long q = 0; q < n; q++) c->psiq[q] = c->scale * c->psiq[q]; /* :849-860 */
+    shift_grad(c, c->psiq, c->gx, c->gy, c->gz);                    /* :864-959 */
+    r3(c, c->psiq, c->psi, T01, T01, T01);                          /* :961-963 */
+    r3(c, c->gx, c->gx, S01, T01, T01);                             /* :965-975 */
+    r3(c, c->gy, c->gy, T01, S01, T01);
+    r3(c, c->gz, c->gz, T01, T01, S01);
+    for (long q = 0; q < n; q++) c->sp2[q] = -c->aLin[q] * c->psiq[q]; /* :980-986 */
+    r3(c, c->sp2, c->sp2, T01, T01, T01);                           /* :988-990 */
+    for (long q = 0; q < n; q++) {                                  /* :994-1015 */
+        double m = (c->sp2[q] - b * pow(c->psi[q], 3) + g * pow(c->psi[q], 5));
+        c->Sx[q] = m * c->gx[q];
+        c->Sy[q] = m * c->gy[q];
+        c->Sz[q] = m * c->gz[q];
+    }
+    r3(c, c->Sx, c->Sx, S10, T10, T10);                             /* :1017-1027 */
+    r3(c, c->Sy, c->Sy, T10, S10, T10);
+    r3(c, c->Sz, c->Sz, T10, T10, S10);
+    stokes(c, 0);                                                   /* :1030-1274 */
+    r3(c, c->vx, c->vx, S01, T01, T01);                             /* :1276-1286 */
+    r3(c, c->vy, c->vy, T01, S01, T01);
+    r3(c, c->vz, c->vz, T01, T01, S01);
+    for (long q = 0; q < n; q++)                                    /* :1290-1303 */
+        c->Nr[q] = b * pow(c->psi[q], 3) - g * pow(c->psi[q], 5) - c->vx[q] * c->gx[q] -
+                   c->vy[q] * c->gy[q] - c->vz[q] * c->gz[q];
+    r3(c, c->Nr, c->Nq, T10, T10, T10);                             /* :1307 */
+    for (long q = 0; q < n; q++)                                    /* :1355-1365 */
+        c->psiq[q] = (c->C1[q] * c->psiq[q] + dtd2 * c->scale * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
+    r3(c, c->psiq, c->psiNew, T01, T01, T01);                       /* :1369 */
+    c->L1 = l1_measure(c, c->psiNew, c->psi);                       /* :1374-1396 */
+    memcpy(c->psi, c->psiNew, sizeof(double) * n);                  /* :1742 */
+}
+
+/* ---------------- quasi: quasi/quasi.cpp:1099-2255 ---------------- */
+static void step_quasi(orc_ctx *c)
+{
+    const long n = c->n;
+    const orc_params *P = &c->p;
+    const double dtd2 = P->dt / 2, b = P->beta, g = P->gamma, ep = P->eps, al = P->alpha;
+    const double q02 = P->q0 * P->q0;
+    c->nloop++;                                                     /* :1103 */
+    memcpy(c->NqPast, c->Nq, sizeof(double) * n);                   /* :1117 (Nl_old = Nl) */
+    for (long q = 0; q < n; q++) c->dfd[q] = al * (q02 - c->mq2[q]) * c->psiq[q]; /* :1121-1131 */
+    r3(c, c->dfd, c->dfd, T01, T01, T01);                           /* :1135-1137 */
+    shift_grad(c, c->psiq, c->gx, c->gy, c->gz);                    /* :1147-1256 */
+    shift_grad(c, c->rhoq, c->rdx, c->rdy, c->rdz);
+    r3(c, c->gx, c->gx, S01, T01, T01);                             /* :1280-1290 */
+    r3(c, c->gy, c->gy, T01, S01, T01);
+    r3(c, c->gz, c->gz, T01, T01, S01);
+    r3(c, c->rdx, c->rdx, S01, T01, T01);                           /* :1294-1304 */
+    r3(c, c->rdy, c->rdy, T01, S01, T01);
+    r3(c, c->rdz, c->rdz, T01, T01, S01);
+    for (long q = 0; q < n; q++)                                    /* :1322-1336 */
+        c->rho[q] = P->kp * sqrt(q02 * pow(c->psi[q], 2) + pow(c->gx[q], 2) + pow(c->gy[q], 2) +
+                                 pow(c->gz[q], 2)) + P->rho0;
+    r3(c, c->rho, c->rhoq, T10, T10, T10);                          /* :1338-1340 */
+    for (long q = 0; q < n; q++)                                    /* :1342-1351 */
+        c->rhoq[q] = c->scale * c->rhoq[q] * exp(-1.57 * 1.57 * c->mq2[q] * 2);
+    r3(c, c->rhoq, c->rho, T01, T01, T01);                          /* :1355-1357 */
+    if (P->loaded && c->nloop == 1) memcpy(c->rho_old, c->rho, sizeof(double) * n); /* :1362-1364 */
+    if (c->nloop > P->divv_switch || P->loaded) {                   /* :1366-1406 */
+        for (long q = 0; q < n; q++) {
+            c->divv[q] = -((c->rho[q] - c->rho_old[q]) / P->dt + c->vx[q] * c->rdx[q] +
+                           c->vy[q] * c->rdy[q] + c->vz[q] * c->rdz[q]) /
+                         (0.5 * (c->rho[q] + c->rho_old[q]));
+            c->lap[q] = c->rho[q] * c->dfd[q];
+        }
+        r3(c, c->lap, c->lap, T10, T10, T10);
+        for (long q = 0; q < n; q++) c->lap[q] = -c->scale * c->mq2[q] * c->lap[q];
+        r3(c, c->lap, c->lap, T01, T01, T01);
+    } else {                                                        /* :1410-1437 */
+        for (long q = 0; q < n; q++) c->lap[q] = -c->mq2[q] * al * (q02 - c->mq2[q]) * c->psiq[q];
+        r3(c, c->lap, c->lap, T01, T01, T01);
+        for (long q = 0; q < n; q++) c->lap[q] = c->rho[q] * c->lap[q];
+    }
+    memcpy(c->rho_old, c->rho, sizeof(double) * n);                 /* :1439 */
+    r3(c, c->divv, c->divv, T10, T10, T10);                         /* :1441-1443 */
+    for (long q = 0; q < n; q++) {                                  /* :1448-1490 */
+        double ps = c->psi[q];
+        c->energy[q] = -0.5 * ep * pow(ps, 2) + 0.5 * pow(c->dfd[q], 2) - 0.25 * b * pow(ps, 4) +
+                       (g / 6) * pow(ps, 6);
+        c->mu[q] = c->lap[q] + c->rho[q] * (c->dfd[q] - ep * ps - b * pow(ps, 3) + g * pow(ps, 5));
+        c->Sx[q] = c->mu[q] * c->gx[q] + c->energy[q] * c->rdx[q];
+        c->Sy[q] = c->mu[q] * c->gy[q] + c->energy[q] * c->rdy[q];
+        c->Sz[q] = c->mu[q] * c->gz[q] + c->energy[q] * c->rdz[q];
+    }
+    r3(c, c->Sx, c->Sx, S10, T10, T10);                             /* :1494-1504 */
+    r3(c, c->Sy, c->Sy, T10, S10, T10);
+    r3(c, c->Sz, c->Sz, T10, T10, S10);
+    /* pressure, quasi/quasi.cpp:1548-1592 (single rank: the back plane is zero, :1546-1550) */
+    for (int i = 0; i < c->nx; i++)
+        for (int j = 0; j < c->ny; j++)
+            for (int k = 0; k < c->nz; k++) {
+                long idx = IDX(c, i, j, k);
+                double Sx = (i > 0) ? c->Sx[IDX(c, i - 1, j, k)] : 0.0;
+                double Sy = (j > 0) ? c->Sy[IDX(c, i, j - 1, k)] : 0.0;
+                double Sz = (k > 0) ? c->Sz[idx - 1] : 0.0;
+                if (i + j + k != 0)
+                    c->p_[idx] = c->scale * (-(c->qx[i] * Sx + c->qy[j] * Sy + c->qz[k] * Sz) / c->mq2[idx] +
+                                             (c->lambda + 2 * P->nu) * c->divv[idx]);
+                else
+                    c->p_[idx] = 0;
+            }
+    r3(c, c->p_, c->p_, T01, T01, T01);                             /* :1590-1592 */
+    stokes(c, 1);                                                   /* :1599-2109 */
+    r3(c, c->vx, c->vx, S01, T01, T01);                             /* :2113-2123 */
+    r3(c, c->vy, c->vy, T01, S01, T01);
+    r3(c, c->vz, c->vz, T01, T01, S01);
+    for (long q = 0; q < n; q++) {                                  /* :2128-2154 */
+        double v = -c->mu[q] - c->vx[q] * c->gx[q] - c->vy[q] * c->gy[q] - c->vz[q] * c->gz[q];
+        if (c->nloop > P->divv_switch + 1)
+            v += (c->p_[q] + c->rho[q] * c->energy[q]) * P->kp *
+                 sqrt(pow(c->rdx[q], 2) + pow(c->rdy[q], 2) + pow(c->rdz[q], 2)) / pow(c->rho[q], 2);
+        c->Nr[q] = v;
+    }
+    r3(c, c->Nr, c->Nq, T10, T10, T10);                             /* :2158-2160 */
+    if (c->nloop == 1) memcpy(c->NqPast, c->Nq, sizeof(double) * n); /* :2162-2164 */
+    for (long q = 0; q < n; q++) {                                  /* :2169-2182 */
+        double old = c->psiq[q];
+        c->psiq[q] = (c->C1[q] * c->psiq[q] - 0.5 * c->psiq_old[q] +
+                      dtd2 * c->scale * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
+        c->psiq_old[q] = old;
+    }
+    memcpy(c->psi_old, c->psi, sizeof(double) * n);                 /* :2186 */
+    r3(c, c->psiq, c->psi, T01, T01, T01);                          /* :2188-2190 */
+    /* diagnostics, quasi/quasi.cpp:2194-2251 */
+    c->L1 = l1_measure(c, c->psi, c->psi_old);
+    double rs = 0.0, es = 0.0;
+    for (long q = 0; q < n; q++) { rs = rs + c->rho[q]; es = es + c->energy[q]; }
+    c->mass = rs * c->dx * c->dx * c->dx;
+    c->en = es * c->dx * c->dx * c->dx;
+}
+
+int orc_step(orc_ctx *c, int nsteps)
+{
+    if (!c || !c->have_psi) return -1;
+    for (int s = 0; s < nsteps; s++) {
+        if (c->p.model == ORC_NOADV) { step_noadv(c); c->nloop++; }
+        else if (c->p.model == ORC_ADV) { step_adv(c); c->nloop++; }
+        else step_quasi(c);
+    }
+    return 0;
+}
+
+int orc_get(const orc_ctx *c, int field, double *out)
+{
+    const double *src = NULL;
+    switch (field) {
+    case ORC_F_PSI: src = c->psi; break;
+    case ORC_F_PSIHAT: src = c->psiq; break;
+    case ORC_F_VX: src = c->vx; break;
+    case ORC_F_VY: src = c->vy; break;
+    case ORC_F_VZ: src = c->vz; break;
+    case ORC_F_GX: src = c->gx; break;
+    case ORC_F_GY: src = c->gy; break;
+    case ORC_F_GZ: src = c->gz; break;
+    case ORC_F_RHO: src = c->rho; break;
+    case ORC_F_P: src = c->p_; break;
+    case ORC_F_DIVV: src = c->divv; break;
+    case ORC_F_MU: src = c->mu; break;
+    case ORC_F_ENERGY: src = c->energy; break;
+    case ORC_F_NHAT: src = c->Nq; break;
+    default: return -1;
+    }
+    if (!src) return -1;
+    memcpy(out, src, sizeof(double) * c->n);
+    return 0;
+}
+
+int orc_diag(const orc_ctx *c, double *d)
+{
+    double s = 0.0;
+    for (long q = 0; q < c->n; q++) s += c->psi[q];
+    d[0] = c->L1;
+    d[1] = c->mass;
+    d[2] = c->en;
+    d[3] = s / (double)c->n;
+    d[4] = (double)c->nloop;
+    return 0;
+}
+
+double orc_free_energy(orc_ctx *c)
+{
+    const long n = c->n;
+    const orc_params *P = &c->p;
+    const double q02 = P->q0 * P->q0;
+    double *ph = dal(n), *f = dal(n);
+    r3(c, c->psi, ph, T10, T10, T10);
+    for (long q = 0; q < n; q++) f[q] = P->alpha * (q02 - c->mq2[q]) * c->scale * ph[q];
+    r3(c, f, f, T01, T01, T01);
+    double es = 0.0;
+    for (long q = 0; q < n; q++) {
+        double ps = c->psi[q];
+        es = es + (-0.5 * P->eps * pow(ps, 2) + 0.5 * pow(f[q], 2) - 0.25 * P->beta * pow(ps, 4) +
+                   (P->gamma / 6) * pow(ps, 6));
+    }
+    free(ph);
+    free(f);
+    return es * c->dx * c->dx * c->dx;
+}
+
+/* Interface trackers:
+ *   mode 0 (flat):  no-adv/cosNoAdvTrackSing.cpp:880-913, adv/cosAdvTrackMult.cpp:1417-1441
+ *   mode 1 (bump):  no-adv/cosNoAdvTrackBump.cpp:936-970 (the upward walk stops at the last
+ *                   index; the reference reads past the end there)
+ *   mode 2 (level): quasi/quasi.cpp:2264-2280 (first value above hi from the top)
+ * The scan runs from the last index of `axis` downwards, as the reference scans k. */
+int orc_track(const orc_ctx *c, int field, int axis, int mode, double hi, double lo, int *idxo,
+              double *poso)
+{
+    const double *f = (field == ORC_F_RHO) ? c->rho : c->psi;
+    if (!f) return -1;
+    int na, nb, nl;
+    long sa, sb, sl;
+    if (axis == 2) { na = c->nx; nb = c->ny; nl = c->nz; sa = (long)c->ny * c->nz; sb = c->nz; sl = 1; }
+    else if (axis == 1) { na = c->nx; nb = c->nz; nl = c->ny; sa = (long)c->ny * c->nz; sb = 1; sl = c->nz; }
+    else { na = c->ny; nb = c->nz; nl = c->nx; sa = c->nz; sb = 1; sl = (long)c->ny * c->nz; }
+    for (int a = 0; a < na; a++)
+        for (int bb = 0; bb < nb; bb++) {
+            const double *col = f + a * sa + bb * sb;
+#define V(t) col[(long)(t) * sl]
+            int found = -1;
+            double pos = NAN;
+            if (mode == 0) {
+                int track = 0;
+                for (int t = nl - 1; t >= 0; t--) {
+                    if (V(t) > hi && track == 0) track = 1;
+                    if (V(t) < lo && track == 1) {
+                        int k2 = t;
+                        if (fabs(V(t)) > fabs(V(t + 1))) k2 = t + 1;
+                        found = k2;
+                        double f0 = V(t), f1 = V(t + 1);
+                        pos = t + (lo - f0) / (f1 - f0);
+                        track = 2;
+                        break;
+                    }
+                }
+            } else if (mode == 1) {
+                for (int t = nl - 1; t >= 0; t--) {
+                    if (fabs(V(t)) > hi) {
+                        int t3 = t;
+                        while (t3 < nl - 1 && fabs(V(t3)) > lo) t3++;
+                        int k2 = t3;
+                        if (t3 + 1 < nl && fabs(V(t3)) > fabs(V(t3 + 1))) k2 = t3 + 1;
+                        found = k2;
+                        if (t3 > t) {
+                            double f0 = fabs(V(t3 - 1)), f1 = fabs(V(t3));
+                            pos = (t3 - 1) + (f0 - lo) / (f0 - f1);
+                        } else {
+                            pos = (double)t3;
+                        }
+                        break;
+                    }
+                }
+            } else {
+                for (int t = nl - 1; t >= 0; t--) {
+                    if (V(t) > hi) {
+                        found = t;
+                        if (t + 1 < nl) {
+                            double f0 = V(t), f1 = V(t + 1);
+                            pos = t + (f0 - hi) / (f0 - f1);
+                        } else {
+                            pos = (double)t;
+                        }
+                        break;
+                    }
+                }
+            }
+#undef V
+            idxo[(long)a * nb + bb] = found;
+            poso[(long)a * nb + bb] = pos;
+        }
+    return 0;
+}
