@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""bench.py -- steps/s of sma-dft's advected (adv) time step at 256^3 on B200.
+
+Metric (the reference's headline path): steps/s at 256^3 adv, mixed precision (FP32 fields,
+FP64 reductions) against the plain FP64 GPU step, with the relative L2 error of psi against
+FP64 stated.  Workload: adv/cosAdvTrackMult.cpp-style step, 256x256x256, dx = lambda0/8,
+dt = 0.02, nu = 1, eps = -0.75, alpha = 1, beta = 2, gamma = 1; synthetic seeded IC
+(smectic layers with 4 focal-conic-like perturbations, smadft_ic_conics).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1).  The path does not shard (one simulation per GPU,
+"replicas only"): every rank runs its own replica, value = all ranks' steps / max time.
+``--impl reference`` times the reference's own loop body (oracle/_ref/adv_ref: the
+reference sources compiled with single-rank MPI / FFTW-r2r shims) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "sma-dft_b200"))
+
+METRIC = "steps/s at 256^3 adv: mixed-prec vs FP64 GPU, at stated L2 err vs FP64"
+N = 256
+CFG = dict(nw=8.0, dt=0.02, eps=-0.75, nu=1.0, alpha=1.0, beta=2.0, gamma=1.0)
+F_ADV = 32          # compulsory full-field transfers per adv step (single-sweep stages)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_run(steps: int, psi0: np.ndarray | None, threads: int):
+    """Run the shimmed reference adv loop at 256^3; returns (steps/s, seconds, kind, sample)."""
+    import oracle
+    shape = (N, N, N)
+    if oracle.reference_available("adv"):
+        with tempfile.TemporaryDirectory() as wd:
+            t0 = time.time()
+            _, _, out = oracle.run_reference("adv", shape, steps, psi0=psi0, workdir=wd,
+                                             threads=threads, **{k: v for k, v in CFG.items()
+                                                                 if k in ("nw", "dt", "eps", "nu")})
+            wall = time.time() - t0
+        m = re.search(r"Finished in ([0-9.eE+-]+) seconds \[Wall Clock\]", out)
+        secs = float(m.group(1)) if m else wall
+        return steps / secs, secs, "reference", (
+            f"{steps} steps of the reference adv loop body at 256^3 (adv/cosAdvTrackMult.cpp, "
+            f"single-rank shim, FFTW replaced by the oracle FP64 r2r), timed by its own wall clock")
+    o = oracle.Oracle(oracle.ADV, shape, **{k: v for k, v in CFG.items()})
+    o.set_psi(psi0)
+    t0 = time.perf_counter()
+    o.step(steps)
+    secs = time.perf_counter() - t0
+    return steps / secs, secs, "port", f"{steps} steps of the FP64 oracle adv step at 256^3"
+
+
+def make_ic():
+    import smadft
+    p = smadft.params(smadft.ADV, (N, N, N), **CFG)
+    return smadft.ic_conics(p, A=1.328, count=4, rmin=3.0, rmax=6.0, noise=1e-3, seed=20240601)
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, 3))
+    psi0 = make_ic()
+    sps, secs, kind, sample = cpu_reference_run(steps, psi0, threads)
+    line = {
+        "metric": METRIC, "value": sps, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": steps, "warmup": 0, "ms_per_step": 1000.0 * secs / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "adv 256^3 time step (cosAdvTrackMult-style), dt=0.02, dx=lambda0/8, nu=1",
+                   "grid": [N, N, N], "host_threads": threads},
+        "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def timed_steps(torch, solver, steps: int, dist, world):
+    """Device time of `steps` loop bodies on the solver's stream, max over ranks."""
+    stream = torch.cuda.ExternalStream(solver.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = solver.launches
+    ev0.record(stream)
+    solver.step(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = solver.launches - l0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms, launches
+
+
+def pass_roofline(torch, smadft, peak):
+    """Per-launch time of the strided (y-axis) DCT-II pass on a 256^3 FP32 field."""
+    p = smadft.params(smadft.ADV, (N, N, N), precision=smadft.FP32, **CFG)
+    with smadft.Solver(p) as s:
+        x = torch.randn((N, N, N), device="cuda", dtype=torch.float32)
+        y = torch.empty_like(x)
+        stream = torch.cuda.ExternalStream(s.stream)
+        out = {}
+        for axis, name in ((2, "z"), (1, "y"), (0, "x")):
+            for _ in range(3):
+                s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, 0)
+            reps = 20
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            for _ in range(reps):
+                s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, 0)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            us = 1000.0 * ev0.elapsed_time(ev1) / reps
+            gbs = 2.0 * 4 * N ** 3 / (us * 1e-6) / 1e9
+            out[name] = {"us": us, "gbs": gbs, "frac": gbs / peak}
+        return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import smadft
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    if not os.path.exists(smadft.LIB_PATH):
+        smadft.build()
+    psi0 = make_ic()
+    peak, peak_kind = peaks()
+    res = {}
+    launches_fp32 = 0
+    clocks = {}
+    for prec, name in ((smadft.FP32, "fp32"), (smadft.FP64, "fp64")):
+        p = smadft.params(smadft.ADV, (N, N, N), precision=prec, device=local_rank, **CFG)
+        with smadft.Solver(p) as s:
+            s.set_psi(psi0)
+            s.step(args.warmup)
+            s.sync()
+            if name == "fp32":
+                with ClockSampler(local_rank) as cs:
+                    ms, launches = timed_steps(torch, s, args.steps, dist, world)
+                clocks = cs.summary()
+                launches_fp32 = launches
+            else:
+                ms, _ = timed_steps(torch, s, args.steps, dist, world)
+            res[name] = {"ms": ms, "psi": s.get("psi")}
+    err = float(np.linalg.norm(res["fp32"]["psi"] - res["fp64"]["psi"]) / np.linalg.norm(res["fp64"]["psi"]))
+    ms_step = res["fp32"]["ms"] / args.steps
+    ms_step64 = res["fp64"]["ms"] / args.steps
+    value = world * args.steps / (res["fp32"]["ms"] / 1000.0)
+
+    # end to end through the public API with host buffers: per step, psi (FP64, pinned host)
+    # goes up, one loop body runs, psi comes back (smadft_step_host)
+    p = smadft.params(smadft.ADV, (N, N, N), precision=smadft.FP32, device=local_rank, **CFG)
+    with smadft.Solver(p) as s:
+        s.set_psi(psi0)
+        host = torch.from_numpy(psi0.copy()).pin_memory()
+        hn = host.numpy()
+        for _ in range(2):
+            s.step_host(hn, 1)
+        e2e_steps = max(3, min(args.steps, 10))
+        stream = torch.cuda.ExternalStream(s.stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(e2e_steps):
+            s.step_host(hn, 1)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+    e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
+
+    passes = pass_roofline(torch, smadft, peak) if rank == 0 else {}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    algo_bytes = 4.0 * N ** 3 * F_ADV
+    achieved = algo_bytes / (ms_step * 1e-3) / 1e9
+    cpu = {}
+    try:
+        sps, secs, kind, sample = cpu_reference_run(2, psi0, os.cpu_count() or 1)
+        cpu = {"value": sps, "unit": "steps/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": sample}
+    except Exception as e:  # reported, not fatal
+        cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("adv_step_fp32_bytes")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "adv 256^3 time step (cosAdvTrackMult-style), dt=0.02, dx=lambda0/8, nu=1, "
+                               "eps=-0.75; FP32 fields, FP64 reductions",
+                   "grid": [N, N, N], "parallelism": f"replicas x{world}",
+                   "l2_flush": "inputs larger than L2 (about 1 GB of fields touched per step)"},
+        "fp64_steps_per_s": world * args.steps / (res["fp64"]["ms"] / 1000.0),
+        "fp64_ms_per_step": ms_step64,
+        "speedup_vs_fp64": ms_step64 / ms_step,
+        "rel_l2_err_vs_fp64": err,
+        "err_after_steps": args.warmup + args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "one adv step (36 r2r_pass_kernel launches); algorithmic bytes "
+                               "= 4 B x 256^3 x 32 compulsory field transfers"},
+        "pass_kernels": passes,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 8 * N ** 3,
+                "d2h_bytes_per_step": 8 * N ** 3},
+        "gpu_launches": launches_fp32,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

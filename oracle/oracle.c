@@ -507,6 +507,7 @@ int orc_track(const orc_ctx *c, int field, int axis, int mode, double hi, double
                 for (int t = nl - 1; t >= 0; t--) {
                     if (V(t) > hi && track == 0) track = 1;
                     if (V(t) < lo && track == 1) {
+                        if (t + 1 >= nl) break;
                         int k2 = t;
                         if (fabs(V(t)) > fabs(V(t + 1))) k2 = t + 1;
                         found = k2;

@@ -1,0 +1,183 @@
+// ctx.cuh -- context, device buffers, per-length FFT plans and launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "r2r_pass.cuh"
+#include "smadft.h"
+
+namespace smadft {
+
+// Field slots (allocated per model; unused slots stay null).
+enum Slot : int {
+    S_PSI = 0, S_PSI2, S_PSIH, S_PSIH_OLD, S_NP, S_TMP,
+    S_GX, S_GY, S_GZ, S_SP2, S_SX, S_SY, S_SZ, S_VX, S_VY, S_VZ,
+    S_RHO, S_RHO_OLD, S_RHOQ, S_DFD, S_RDX, S_RDY, S_RDZ, S_LAP, S_DIVV, S_P, S_MU, S_EN,
+    S_COUNT
+};
+
+struct PlanDev {
+    int nst;
+    int radix[kMaxStages];
+    void *w;   // cpx<T>[n]
+    void *h;   // cpx<T>[n]
+};
+
+// Model constants handed to device functors by value.
+template <typename T>
+struct Spec {
+    const T *qx, *qy, *qz, *sx, *sy, *sz;   // DCT / DST wavenumbers per axis
+    const T *ex, *ey, *ez;                   // exp(-2 * 1.57^2 q^2) per axis (quasi filter)
+    T eps, alpha, beta, gamma, q02, dtd2, dt, scale, nu;
+    T rho_m, lam, kp, rho0;
+    int nx, ny, nz;
+    long long nyz;
+    __device__ __forceinline__ T mq2(int i, int j, int k) const
+    {
+        return qx[i] * qx[i] + qy[j] * qy[j] + qz[k] * qz[k];
+    }
+    // L(q) = eps - alpha (q^2 - q0^2)^2   (no-adv/cosNoAdvTrackSing.cpp:598-600)
+    __device__ __forceinline__ T alin(int i, int j, int k) const
+    {
+        T d = mq2(i, j, k) - q02;
+        return eps - alpha * (d * d);
+    }
+};
+
+struct Ctx {
+    smadft_params p;
+    bool f32 = false;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    Geom g{};
+    long long n = 0;
+    double Lx = 0, Ly = 0, Lz = 0, dx = 0, dy = 0, dz = 0, scale = 0;
+    std::string err;
+    void *slot[S_COUNT] = {};
+    size_t esize = 8;
+    void *tables = nullptr;     // qx qy qz sx sy sz ex ey ez (T), contiguous
+    size_t off[9] = {};
+    std::map<int, PlanDev> plans;
+    double *red = nullptr;      // reduction partials (device)
+    double *red_out = nullptr;  // final sums (device)
+    int red_blocks = 0;
+    long long steps = 0;        // loop iterations since set_psi
+    bool have_psi = false;
+    bool psi_current = false;   // adv: S_PSI holds iCT(psihat) of the current state
+    long long launches = 0;     // kernels launched by this context
+    double *stage = nullptr;    // FP64 staging field for host-psi steps (allocated on first use)
+
+    template <typename T>
+    T *f(int s) const { return reinterpret_cast<T *>(slot[s]); }
+    template <typename T>
+    const T *tab(int which) const
+    {
+        return reinterpret_cast<const T *>(reinterpret_cast<const char *>(tables) + off[which]);
+    }
+};
+
+#define SMADFT_CUDA(call)                                                            \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            c.err = std::string(#call) + ": " + cudaGetErrorString(e_);              \
+            return SMADFT_ERR_CUDA;                                                  \
+        }                                                                            \
+    } while (0)
+
+template <typename T>
+Spec<T> make_spec(const Ctx &c)
+{
+    Spec<T> s;
+    s.qx = c.tab<T>(0); s.qy = c.tab<T>(1); s.qz = c.tab<T>(2);
+    s.sx = c.tab<T>(3); s.sy = c.tab<T>(4); s.sz = c.tab<T>(5);
+    s.ex = c.tab<T>(6); s.ey = c.tab<T>(7); s.ez = c.tab<T>(8);
+    const smadft_params &p = c.p;
+    s.eps = T(p.eps); s.alpha = T(p.alpha); s.beta = T(p.beta); s.gamma = T(p.gamma);
+    s.q02 = T(p.q0 * p.q0); s.dtd2 = T(p.dt / 2); s.dt = T(p.dt); s.scale = T(c.scale);
+    s.nu = T(p.nu);
+    double rho_s = p.kp * p.amp + p.rho0;       // quasi/quasi.cpp:244-245
+    s.rho_m = T(rho_s / 2); s.lam = T(-2 * p.nu / 3); s.kp = T(p.kp); s.rho0 = T(p.rho0);
+    s.nx = c.g.nx; s.ny = c.g.ny; s.nz = c.g.nz; s.nyz = c.g.nyz;
+    return s;
+}
+
+// Tile width: one 128-byte row segment per tile row.
+template <typename T>
+constexpr int tile_w() { return sizeof(T) == 4 ? 32 : 16; }
+
+template <typename T, class LD, class ST>
+int launch_pass(Ctx &c, int axis, int kind, LD ld, ST st)
+{
+    const int n = axis == 0 ? c.g.nx : (axis == 1 ? c.g.ny : c.g.nz);
+    const PlanDev &pd = c.plans.at(n);
+    PassArgs<T> a;
+    a.g = c.g;
+    a.axis = axis;
+    a.kind = kind;
+    a.W = tile_w<T>();
+    a.ld = n;
+    a.P.n = n;
+    a.P.nst = pd.nst;
+    for (int s = 0; s < kMaxStages; s++) a.P.radix[s] = pd.radix[s];
+    a.P.w = reinterpret_cast<const cpx<T> *>(pd.w);
+    a.P.h = reinterpret_cast<const cpx<T> *>(pd.h);
+    long long tiles;
+    if (axis == 2) {
+        a.tiles_b = 1;
+        tiles = ((long long)c.g.nx * c.g.ny + a.W - 1) / a.W;
+    } else {
+        a.tiles_b = (c.g.nz + a.W - 1) / a.W;
+        tiles = (long long)(axis == 1 ? c.g.nx : c.g.ny) * a.tiles_b;
+    }
+    const size_t smem = 2 * (size_t)(a.W / 2) * a.ld * sizeof(cpx<T>);
+    static size_t attr_set = 0;   // largest opt-in so far, per template instantiation
+    if (smem > attr_set) {
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_pass_kernel<T, LD, ST>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = smem;
+    }
+    r2r_pass_kernel<T, LD, ST><<<(unsigned)tiles, 256, smem, c.stream>>>(a, ld, st);
+    SMADFT_CUDA(cudaGetLastError());
+    c.launches++;
+    return SMADFT_OK;
+}
+
+// Element-wise precision conversion (host-psi steps).
+template <typename S, typename D>
+__global__ void convert_kernel(const S *__restrict__ src, D *__restrict__ dst, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) dst[q] = D(src[q]);
+}
+
+template <typename S, typename D>
+int convert(Ctx &c, const S *src, D *dst)
+{
+    convert_kernel<S, D><<<1184, 256, 0, c.stream>>>(src, dst, c.n);
+    SMADFT_CUDA(cudaGetLastError());
+    c.launches++;
+    return SMADFT_OK;
+}
+
+// 3-D transform: z pass (custom loader) -> y pass -> x pass (custom storer), in place on
+// the scratch field.
+template <typename T, class LD, class ST>
+int r2r3d(Ctx &c, int kx, int ky, int kz, LD ld, ST st)
+{
+    T *tmp = c.f<T>(S_TMP);
+    int rc = launch_pass<T>(c, 2, kz, ld, StoreArr<T>{tmp});
+    if (rc) return rc;
+    rc = launch_pass<T>(c, 1, ky, LoadArr<T>{tmp}, StoreArr<T>{tmp});
+    if (rc) return rc;
+    return launch_pass<T>(c, 0, kx, LoadArr<T>{tmp}, st);
+}
+
+}  // namespace smadft

@@ -1,0 +1,258 @@
+// quasi.cuh -- the quasi-incompressible loop body (quasi/quasi.cpp:1099-2190) as fused
+// r2r passes.  Density law, Gaussian filter, div v from the mass balance, pressure,
+// solenoidal + irrotational velocity and the BDF2-like update all ride in the loaders and
+// storers of the 21 transforms the reference runs per step.
+#pragma once
+
+#include "models.cuh"
+#include "reduce.cuh"
+
+namespace smadft {
+
+// f' = alpha (q0^2 - q^2) psihat (quasi/quasi.cpp:1121-1131)
+template <typename T>
+struct LdDfd {
+    Spec<T> s;
+    const T *__restrict__ ph;
+    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    {
+        return s.alpha * (s.q02 - s.mq2(i, j, k)) * ph[q];
+    }
+};
+
+// -q^2 alpha (q0^2 - q^2) psihat (quasi/quasi.cpp:1414-1420)
+template <typename T>
+struct LdLapDfd {
+    Spec<T> s;
+    const T *__restrict__ ph;
+    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    {
+        T m = s.mq2(i, j, k);
+        return -m * s.alpha * (s.q02 - m) * ph[q];
+    }
+};
+
+// rho = kp sqrt(q0^2 psi^2 + |grad psi|^2) + rho0 (quasi/quasi.cpp:1322-1336)
+template <typename T>
+struct LdRhoRaw {
+    const T *__restrict__ psi, *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
+    T kp, rho0, q02;
+    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    {
+        T p = psi[q], a = gx[q], b = gy[q], c = gz[q];
+        return kp * sqrt(q02 * (p * p) + a * a + b * b + c * c) + rho0;
+    }
+};
+
+// rhohat = scale REDFT10^3(rho) exp(-2 1.57^2 q^2) (quasi/quasi.cpp:1342-1351)
+template <typename T>
+struct StFilter {
+    Spec<T> s;
+    T *__restrict__ out;
+    __device__ __forceinline__ void operator()(long long q, int i, int j, int k, T v) const
+    {
+        out[q] = (s.scale * v) * (s.ex[i] * s.ey[j] * s.ez[k]);
+    }
+};
+
+// div v = -((rho - rho_old)/dt + v . grad rho) / (0.5 (rho + rho_old)) (quasi/quasi.cpp:1370-1377)
+template <typename T>
+struct LdDivv {
+    const T *__restrict__ rho, *__restrict__ ro, *__restrict__ vx, *__restrict__ vy, *__restrict__ vz;
+    const T *__restrict__ rx, *__restrict__ ry, *__restrict__ rz;
+    T dt;
+    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    {
+        T r = rho[q], o = ro[q];
+        return -((r - o) / dt + vx[q] * rx[q] + vy[q] * ry[q] + vz[q] * rz[q]) / (T(0.5) * (r + o));
+    }
+};
+
+template <typename T>
+struct LdMul {
+    const T *__restrict__ a, *__restrict__ b;
+    __device__ __forceinline__ T operator()(long long q, int, int, int) const { return a[q] * b[q]; }
+};
+
+// lap <- -scale q^2 REDFT10^3(rho f') (quasi/quasi.cpp:1392-1400)
+template <typename T>
+struct StLapSpec {
+    Spec<T> s;
+    T *__restrict__ out;
+    __device__ __forceinline__ void operator()(long long q, int i, int j, int k, T v) const
+    {
+        out[q] = -s.scale * s.mq2(i, j, k) * v;
+    }
+};
+
+// e, mu and S_c = mu d_c psi + e d_c rho (quasi/quasi.cpp:1448-1490).  AX == 0 also stores mu
+// and e; lap_rho == 1 multiplies the relaxation-branch Laplacian by rho (:1429-1435).
+template <typename T, int AX>
+struct LdQForce {
+    const T *__restrict__ psi, *__restrict__ dfd, *__restrict__ lap, *__restrict__ rho;
+    const T *__restrict__ g, *__restrict__ r;
+    T *__restrict__ mu_out, *__restrict__ en_out;
+    T eps, beta, gamma;
+    int lap_rho;
+    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    {
+        T ps = psi[q], f = dfd[q], rh = rho[q];
+        T p2 = ps * ps, p3 = p2 * ps, p4 = p2 * p2;
+        T e = T(-0.5) * eps * p2 + T(0.5) * (f * f) - T(0.25) * beta * p4 + (gamma / T(6)) * (p4 * p2);
+        T lv = lap_rho ? rh * lap[q] : lap[q];
+        T m = lv + rh * (f - eps * ps - beta * p3 + gamma * (p3 * p2));
+        if (AX == 0) {
+            mu_out[q] = m;
+            en_out[q] = e;
+        }
+        return m * g[q] + e * r[q];
+    }
+};
+
+// p = scale(-(q . S[-1 shifts]) / q^2 + (lambda + 2 nu) divv), p(0,0,0) = 0 (quasi/quasi.cpp:1553-1588)
+template <typename T>
+struct LdPressure {
+    Spec<T> s;
+    const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz, *__restrict__ dv;
+    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    {
+        if (i + j + k == 0) return T(0);
+        T sx = (i > 0) ? Sx[q - s.nyz] : T(0);
+        T sy = (j > 0) ? Sy[q - s.nz] : T(0);
+        T sz = (k > 0) ? Sz[q - 1] : T(0);
+        return s.scale * (-(s.qx[i] * sx + s.qy[j] * sy + s.qz[k] * sz) / s.mq2(i, j, k) +
+                          (s.lam + T(2) * s.nu) * dv[q]);
+    }
+};
+
+// Nl = -mu - v . grad psi [+ (p + rho e) kp |grad rho| / rho^2 after the switch]
+// (quasi/quasi.cpp:2128-2154)
+template <typename T>
+struct LdQN {
+    const T *__restrict__ mu, *__restrict__ vx, *__restrict__ vy, *__restrict__ vz;
+    const T *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
+    const T *__restrict__ p, *__restrict__ rho, *__restrict__ en;
+    const T *__restrict__ rx, *__restrict__ ry, *__restrict__ rz;
+    T kp;
+    int extra;
+    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    {
+        T v = -mu[q] - vx[q] * gx[q] - vy[q] * gy[q] - vz[q] * gz[q];
+        if (extra) {
+            T a = rx[q], b = ry[q], c = rz[q], r = rho[q];
+            v += (p[q] + r * en[q]) * kp * sqrt(a * a + b * b + c * c) / (r * r);
+        }
+        return v;
+    }
+};
+
+// psihat <- (C1 psihat - psihat_old/2 + dt/2 scale (3 N - Nprev)) / C2,
+// C1 = 2 - dt rho_m L, C2 = 1.5 - dt rho_m L; first step uses Nprev = N (quasi/quasi.cpp:2162-2182)
+template <typename T>
+struct StUpdBDF {
+    Spec<T> s;
+    T *__restrict__ ph, *__restrict__ pho, *__restrict__ np;
+    int first;
+    __device__ __forceinline__ void operator()(long long q, int i, int j, int k, T v) const
+    {
+        T al = s.alin(i, j, k);
+        T c1 = T(2) - s.dt * s.rho_m * al, c2 = T(1.5) - s.dt * s.rho_m * al;
+        T npv = first ? v : np[q];
+        T old = ph[q];
+        ph[q] = (c1 * old - T(0.5) * pho[q] + s.dtd2 * s.scale * (T(3) * v - npv)) / c2;
+        pho[q] = old;
+        np[q] = v;
+    }
+};
+
+template <typename T>
+int quasi_pre_loop(Ctx &c)
+{
+    Spec<T> s = make_spec<T>(c);
+    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH);
+    int rc;
+    // psihat = scale CT(psi); psi = iCT(psihat); psihat_old = psihat (quasi/quasi.cpp:990-1034)
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, s.scale}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{psi}))) return rc;
+    SMADFT_CUDA(cudaMemcpyAsync(c.slot[S_PSIH_OLD], ph, sizeof(T) * c.n, cudaMemcpyDeviceToDevice, c.stream));
+    return SMADFT_OK;
+}
+
+template <typename T>
+int quasi_step(Ctx &c, long long nloop, bool keep_old)
+{
+    Spec<T> s = make_spec<T>(c);
+    const smadft_params &P = c.p;
+    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *pho = c.f<T>(S_PSIH_OLD), *np = c.f<T>(S_NP);
+    T *gx = c.f<T>(S_GX), *gy = c.f<T>(S_GY), *gz = c.f<T>(S_GZ);
+    T *rx = c.f<T>(S_RDX), *ry = c.f<T>(S_RDY), *rz = c.f<T>(S_RDZ);
+    T *rho = c.f<T>(S_RHO), *ro = c.f<T>(S_RHO_OLD), *rq = c.f<T>(S_RHOQ);
+    T *dfd = c.f<T>(S_DFD), *lap = c.f<T>(S_LAP), *dv = c.f<T>(S_DIVV), *pp = c.f<T>(S_P);
+    T *mu = c.f<T>(S_MU), *en = c.f<T>(S_EN);
+    T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
+    T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
+    int rc;
+    // f', grad psi, grad rho (quasi/quasi.cpp:1121-1304)
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdDfd<T>{s, ph}, StoreArr<T>{dfd}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdGrad<T, 0>{s, ph}, StoreArr<T>{gx}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdGrad<T, 1>{s, ph}, StoreArr<T>{gy}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdGrad<T, 2>{s, ph}, StoreArr<T>{gz}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdGrad<T, 0>{s, rq}, StoreArr<T>{rx}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdGrad<T, 1>{s, rq}, StoreArr<T>{ry}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdGrad<T, 2>{s, rq}, StoreArr<T>{rz}))) return rc;
+    // density law + filter (:1322-1357)
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdRhoRaw<T>{psi, gx, gy, gz, s.kp, s.rho0, s.q02},
+                       StFilter<T>{s, rq}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{rq}, StoreArr<T>{rho}))) return rc;
+    if (P.loaded && nloop == 1)
+        SMADFT_CUDA(cudaMemcpyAsync(ro, rho, sizeof(T) * c.n, cudaMemcpyDeviceToDevice, c.stream));
+    int lap_rho;
+    if (nloop > P.divv_switch || P.loaded) {   // :1366-1406
+        if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdDivv<T>{rho, ro, vx, vy, vz, rx, ry, rz, s.dt},
+                           StoreArr<T>{dv}))) return rc;
+        if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdMul<T>{rho, dfd}, StLapSpec<T>{s, lap}))) return rc;
+        if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{lap}, StoreArr<T>{lap}))) return rc;
+        lap_rho = 0;
+    } else {                                   // :1410-1437 (div v stays 0 before the switch)
+        SMADFT_CUDA(cudaMemsetAsync(dv, 0, sizeof(T) * c.n, c.stream));
+        if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdLapDfd<T>{s, ph}, StoreArr<T>{lap}))) return rc;
+        lap_rho = 1;
+    }
+    SMADFT_CUDA(cudaMemcpyAsync(ro, rho, sizeof(T) * c.n, cudaMemcpyDeviceToDevice, c.stream));  // :1439
+    // forces (:1448-1504); the x loader also stores mu and e
+    if ((rc = r2r3d<T>(c, K_DST2, K_DCT2, K_DCT2,
+                       LdQForce<T, 0>{psi, dfd, lap, rho, gx, rx, mu, en, s.eps, s.beta, s.gamma, lap_rho},
+                       StoreArr<T>{Sx}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DST2, K_DCT2,
+                       LdQForce<T, 1>{psi, dfd, lap, rho, gy, ry, nullptr, nullptr, s.eps, s.beta, s.gamma, lap_rho},
+                       StoreArr<T>{Sy}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DST2,
+                       LdQForce<T, 2>{psi, dfd, lap, rho, gz, rz, nullptr, nullptr, s.eps, s.beta, s.gamma, lap_rho},
+                       StoreArr<T>{Sz}))) return rc;
+    // pressure (:1510-1592)
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdPressure<T>{s, Sx, Sy, Sz, dv}, StoreArr<T>{pp}))) return rc;
+    // velocity = solenoidal + irrotational (:1599-2123)
+    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdStokes<T, 0, true>{s, Sx, Sy, Sz, dv}, StoreArr<T>{vx}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdStokes<T, 1, true>{s, Sx, Sy, Sz, dv}, StoreArr<T>{vy}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdStokes<T, 2, true>{s, Sx, Sy, Sz, dv}, StoreArr<T>{vz}))) return rc;
+    // N and the BDF2-like update (:2128-2182)
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
+                       LdQN<T>{mu, vx, vy, vz, gx, gy, gz, pp, rho, en, rx, ry, rz, s.kp,
+                               (int)(nloop > P.divv_switch + 1)},
+                       StUpdBDF<T>{s, ph, pho, np, (int)(nloop == 1)}))) return rc;
+    // psi = iCT(psihat) (:2186-2190)
+    T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
+    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{dst});
+}
+
+template <typename T>
+int reduce_mass_energy(Ctx &c, double *ms)
+{
+    double out[kRedVals];
+    int rc = run_reduce(c, RedSum2<T>{c.f<T>(S_RHO), c.f<T>(S_EN)}, out);
+    ms[0] = out[0];
+    ms[1] = out[1];
+    return rc;
+}
+
+}  // namespace smadft

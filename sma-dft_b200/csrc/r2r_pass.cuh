@@ -1,0 +1,158 @@
+// r2r_pass.cuh -- one axis pass of a 3-D r2r transform over an nx*ny*nz field
+// (layout idx = (i*ny + j)*nz + k, the reference's x-slab order, z contiguous).
+//
+// A CTA owns a tile of W lines: for the z axis W consecutive rows (contiguous), for the
+// y and x axes W consecutive k-columns (so every global access is a coalesced run along
+// z).  The tile is staged in shared memory as W/2 complex lines, transformed, and written
+// back.  The first pass of a 3-D transform reads through a Loader functor (it computes the
+// transform input from any number of fields: nonlinearity, spectral update, index-shifted
+// gradient spectra, Stokes projection ...); the last pass writes through a Storer functor.
+// Passes are in place on the tile, so a 3-D transform needs one scratch field.
+#pragma once
+
+#include "fft_tile.cuh"
+
+namespace smadft {
+
+struct Geom {
+    int nx, ny, nz;
+    long long nyz;   // ny * nz
+};
+
+template <typename T>
+struct PassArgs {
+    Geom g;
+    int axis;        // 0 = x, 1 = y, 2 = z
+    int kind;        // R2RKind
+    int W;           // lines per tile (even)
+    int ld;          // shared-memory line stride (complex elements)
+    int tiles_b;     // tiles along the second tile coordinate
+    LinePlan<T> P;
+};
+
+// Element coordinates for tile-local (t = position along the line, w = line in tile).
+struct ElemPos {
+    long long idx;
+    int i, j, k;
+    bool valid;
+};
+
+template <typename T>
+__device__ __forceinline__ ElemPos elem_pos(const PassArgs<T> &a, int t, int w)
+{
+    ElemPos e;
+    const Geom &g = a.g;
+    if (a.axis == 2) {
+        long long line = (long long)blockIdx.x * a.W + w;    // line = i*ny + j
+        e.valid = line < (long long)g.nx * g.ny;
+        int i = (int)(line / g.ny);
+        int j = (int)(line - (long long)i * g.ny);
+        e.i = i; e.j = j; e.k = t;
+        e.idx = line * g.nz + t;
+    } else {
+        const int tb = blockIdx.x % a.tiles_b;
+        const int ta = blockIdx.x / a.tiles_b;
+        const int k = tb * a.W + w;
+        e.valid = k < g.nz;
+        e.k = k;
+        if (a.axis == 1) {  // lines (i, k), t = j
+            e.i = ta; e.j = t;
+        } else {            // lines (j, k), t = i
+            e.j = ta; e.i = t;
+        }
+        e.idx = ((long long)e.i * g.ny + e.j) * g.nz + k;
+    }
+    return e;
+}
+
+// Identity loader / storer on a plain array.
+template <typename T>
+struct LoadArr {
+    const T *__restrict__ p;
+    __device__ __forceinline__ T operator()(long long idx, int, int, int) const { return p[idx]; }
+};
+template <typename T>
+struct StoreArr {
+    T *__restrict__ p;
+    __device__ __forceinline__ void operator()(long long idx, int, int, int, T v) const { p[idx] = v; }
+};
+
+template <typename T, class LD, class ST>
+__global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T> *bufA = reinterpret_cast<cpx<T> *>(smem_raw);
+    const int n = a.P.n;
+    const int W = a.W;
+    const int nl = W >> 1;                 // complex lines in the tile
+    cpx<T> *bufB = bufA + nl * a.ld;
+    T *realA = reinterpret_cast<T *>(bufA);
+    const int kind = a.kind;
+    const bool fwd = (kind == K_DCT2 || kind == K_DST2);
+    const int total = n * W;
+
+    // ---- load: input permutation per kind --------------------------------------------
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        int t, w;
+        if (a.axis == 2) { t = e % n; w = e / n; }
+        else { w = e % W; t = e / W; }
+        ElemPos p = elem_pos(a, t, w);
+        T v = p.valid ? ld(p.idx, p.i, p.j, p.k) : T(0);
+        int pos;
+        if (kind == K_DCT2) pos = makhoul_pos(t, n);
+        else if (kind == K_DST2) { pos = makhoul_pos(t, n); if (t & 1) v = -v; }
+        else if (kind == K_DCT3) pos = t;
+        else pos = n - 1 - t;
+        realA[2 * ((w >> 1) * a.ld + pos) + (w & 1)] = v;
+    }
+    __syncthreads();
+
+    cpx<T> *res;
+    if (fwd) {
+        res = fft_lines<T, false>(bufA, bufB, nl, a.ld, a.P);
+    } else {
+        // DCT-III pre-twiddle: Z_t = V_A[t] + i V_B[t],
+        // V[t] = exp(+i pi t/2n) (X_t - i X_{n-t}), X_n = 0
+        for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+            const int c = e / n;
+            const int t = e - c * n;
+            const cpx<T> *L = bufA + c * a.ld;
+            cpx<T> xt = L[t];
+            cpx<T> xm = (t == 0) ? cpx<T>{T(0), T(0)} : L[n - t];
+            cpx<T> hh = a.P.h[t];   // (cos, sin) of pi t / 2n
+            T cc = hh.x, ss = hh.y;
+            // V_A = (c A_t + s A_m) + i (s A_t - c A_m), same for B; Z = V_A + i V_B
+            T var = cc * xt.x + ss * xm.x, vai = ss * xt.x - cc * xm.x;
+            T vbr = cc * xt.y + ss * xm.y, vbi = ss * xt.y - cc * xm.y;
+            bufB[c * a.ld + t] = {var - vbi, vai + vbr};
+        }
+        __syncthreads();
+        res = fft_lines<T, true>(bufB, bufA, nl, a.ld, a.P);
+    }
+
+    // ---- store: output permutation / post-twiddle per kind --------------------------
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        int o, w;
+        if (a.axis == 2) { o = e % n; w = e / n; }
+        else { w = e % W; o = e / W; }
+        ElemPos p = elem_pos(a, o, w);
+        const cpx<T> *L = res + (w >> 1) * a.ld;
+        T v;
+        if (fwd) {
+            const int k = (kind == K_DCT2) ? o : (n - 1 - o);
+            cpx<T> zk = L[k];
+            cpx<T> zm = L[k == 0 ? 0 : n - k];
+            cpx<T> hh = a.P.h[k];
+            T cc = hh.x, ss = hh.y;
+            if ((w & 1) == 0) v = cc * (zk.x + zm.x) + ss * (zk.y - zm.y);
+            else v = cc * (zk.y + zm.y) - ss * (zk.x - zm.x);
+        } else {
+            cpx<T> z = L[makhoul_pos(o, n)];
+            v = (w & 1) ? z.y : z.x;
+            if (kind == K_DST3 && (o & 1)) v = -v;
+        }
+        if (p.valid) st(p.idx, p.i, p.j, p.k, v);
+    }
+}
+
+}  // namespace smadft

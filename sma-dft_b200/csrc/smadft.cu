@@ -1,0 +1,600 @@
+// smadft.cu -- C ABI implementation: context set-up, the per-model loop bodies, FP64
+// diagnostics, interface tracker and checkpoints.  See include/smadft.h for the contract.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ctx.cuh"
+#include "models.cuh"
+#include "quasi.cuh"
+#include "reduce.cuh"
+#include "smadft.h"
+
+using namespace smadft;
+
+struct smadft_ctx {
+    Ctx c;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_variant = -1;
+};
+
+namespace {
+
+int fail(Ctx &c, int code, const std::string &msg)
+{
+    c.err = msg;
+    return code;
+}
+
+bool factor_ok(int n)
+{
+    if (n < 2 || (n & 1)) return false;
+    while (n % 2 == 0) n /= 2;
+    while (n % 3 == 0) n /= 3;
+    while (n % 5 == 0) n /= 5;
+    return n == 1;
+}
+
+// radix sequence: 4s, then a 2, then 3s and 5s (same factor order as the oracle)
+void make_radices(int n, PlanDev &pd)
+{
+    int m = n, s = 0;
+    while (m % 4 == 0) { pd.radix[s++] = 4; m /= 4; }
+    while (m % 2 == 0) { pd.radix[s++] = 2; m /= 2; }
+    while (m % 3 == 0) { pd.radix[s++] = 3; m /= 3; }
+    while (m % 5 == 0) { pd.radix[s++] = 5; m /= 5; }
+    pd.nst = s;
+    for (; s < kMaxStages; s++) pd.radix[s] = 1;
+}
+
+template <typename T>
+int upload_plan(Ctx &c, int n)
+{
+    if (c.plans.count(n)) return SMADFT_OK;
+    PlanDev pd{};
+    make_radices(n, pd);
+    std::vector<cpx<T>> w(n), h(n);
+    for (int m = 0; m < n; m++) {
+        double a = 2.0 * M_PI * (double)m / (double)n;
+        w[m] = {T(std::cos(a)), T(-std::sin(a))};
+        double b = M_PI * (double)m / (2.0 * (double)n);
+        h[m] = {T(std::cos(b)), T(std::sin(b))};
+    }
+    SMADFT_CUDA(cudaMalloc(&pd.w, sizeof(cpx<T>) * n));
+    SMADFT_CUDA(cudaMalloc(&pd.h, sizeof(cpx<T>) * n));
+    SMADFT_CUDA(cudaMemcpy(pd.w, w.data(), sizeof(cpx<T>) * n, cudaMemcpyHostToDevice));
+    SMADFT_CUDA(cudaMemcpy(pd.h, h.data(), sizeof(cpx<T>) * n, cudaMemcpyHostToDevice));
+    c.plans[n] = pd;
+    return SMADFT_OK;
+}
+
+// Wavenumber tables exactly as the reference forms them (no-adv/cosNoAdvTrackSing.cpp:
+// 309-324, adv/cosAdvTrackMult.cpp:386-401), then converted to the compute type.
+template <typename T>
+int upload_tables(Ctx &c)
+{
+    const int nx = c.g.nx, ny = c.g.ny, nz = c.g.nz;
+    std::vector<double> qx(nx), qy(ny), qz(nz), sx(nx), sy(ny), sz(nz), ex(nx), ey(ny), ez(nz);
+    for (int i = 0; i < nx; i++) { qx[i] = 1.0 * M_PI * i / (c.dx * nx); sx[i] = 1.0 * M_PI * (i + 1) / (c.dx * nx); }
+    for (int j = 0; j < ny; j++) { qy[j] = M_PI * (j) / (c.dy * ny); sy[j] = M_PI * (j + 1) / (c.dy * ny); }
+    for (int k = 0; k < nz; k++) { qz[k] = M_PI * (k) / (c.dz * nz); sz[k] = M_PI * (k + 1) / (c.dz * nz); }
+    // quasi Gaussian filter exp(-1.57^2 q^2 2) (quasi/quasi.cpp:1349), separable per axis
+    const double fk = 1.57 * 1.57 * 2;
+    for (int i = 0; i < nx; i++) ex[i] = std::exp(-fk * qx[i] * qx[i]);
+    for (int j = 0; j < ny; j++) ey[j] = std::exp(-fk * qy[j] * qy[j]);
+    for (int k = 0; k < nz; k++) ez[k] = std::exp(-fk * qz[k] * qz[k]);
+    const std::vector<double> *t[9] = {&qx, &qy, &qz, &sx, &sy, &sz, &ex, &ey, &ez};
+    std::vector<T> all;
+    for (int q = 0; q < 9; q++) {
+        c.off[q] = all.size() * sizeof(T);
+        for (double v : *t[q]) all.push_back(T(v));
+    }
+    SMADFT_CUDA(cudaMalloc(&c.tables, all.size() * sizeof(T)));
+    SMADFT_CUDA(cudaMemcpy(c.tables, all.data(), all.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SMADFT_OK;
+}
+
+std::vector<int> slots_for(int model)
+{
+    std::vector<int> s = {S_PSI, S_PSI2, S_PSIH, S_NP, S_TMP};
+    if (model != SMADFT_MODEL_NOADV) {
+        for (int q : {S_GX, S_GY, S_GZ, S_SP2, S_SX, S_SY, S_SZ, S_VX, S_VY, S_VZ}) s.push_back(q);
+    }
+    if (model == SMADFT_MODEL_QUASI) {
+        for (int q : {S_PSIH_OLD, S_RHO, S_RHO_OLD, S_RHOQ, S_DFD, S_RDX, S_RDY, S_RDZ, S_LAP,
+                      S_DIVV, S_P, S_MU, S_EN})
+            s.push_back(q);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- steps ---------------
+template <typename T>
+int noadv_step(Ctx &c, bool keep_old)
+{
+    Spec<T> s = make_spec<T>(c);
+    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
+    // N^n = REDFT10^3(beta psi^3 - gamma psi^5), fused CN/AB2 update of psihat
+    int rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
+                      StUpdCN<T>{s, ph, np});
+    if (rc) return rc;
+    // psi^{n+1} = REDFT01^3 psihat (into the second buffer when the old psi is needed)
+    T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
+    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{dst});
+}
+
+template <typename T>
+int adv_step(Ctx &c)
+{
+    Spec<T> s = make_spec<T>(c);
+    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
+    T *gx = c.f<T>(S_GX), *gy = c.f<T>(S_GY), *gz = c.f<T>(S_GZ), *sp2 = c.f<T>(S_SP2);
+    T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
+    T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
+    int rc;
+    // psi and grad psi from psihat (adv/cosAdvTrackMult.cpp:904-975)
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{psi}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdGrad<T, 0>{s, ph}, StoreArr<T>{gx}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdGrad<T, 1>{s, ph}, StoreArr<T>{gy}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdGrad<T, 2>{s, ph}, StoreArr<T>{gz}))) return rc;
+    // Sp2 = iCT(-L psihat) (:980-991)
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdNegLin<T>{s, ph}, StoreArr<T>{sp2}))) return rc;
+    // force spectra S_c = ST_c(mu d_c psi) (:996-1027)
+    if ((rc = r2r3d<T>(c, K_DST2, K_DCT2, K_DCT2, LdForce<T>{psi, sp2, gx, s.beta, s.gamma}, StoreArr<T>{Sx}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DST2, K_DCT2, LdForce<T>{psi, sp2, gy, s.beta, s.gamma}, StoreArr<T>{Sy}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DST2, LdForce<T>{psi, sp2, gz, s.beta, s.gamma}, StoreArr<T>{Sz}))) return rc;
+    // Stokes velocity (:1030-1286)
+    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vx}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vy}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vz}))) return rc;
+    // N = beta psi^3 - gamma psi^5 - v.grad psi, CN/AB2 update (:1290-1365)
+    return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
+                    LdAdvN<T>{psi, vx, vy, vz, gx, gy, gz, s.beta, s.gamma}, StUpdCN<T>{s, ph, np});
+}
+
+template <typename T>
+int refresh_psi(Ctx &c, T *dst)
+{
+    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{c.f<T>(S_PSIH)}, StoreArr<T>{dst});
+}
+
+template <typename T>
+int pre_loop(Ctx &c)
+{
+    Spec<T> s = make_spec<T>(c);
+    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
+    int rc;
+    if (c.p.model == SMADFT_MODEL_QUASI) return quasi_pre_loop<T>(c);
+    // psihat = scale REDFT10^3 psi ; Nprev = REDFT10^3(beta psi^3 - gamma psi^5) (no advection)
+    // no-adv/cosNoAdvTrackSing.cpp:618-635, adv/cosAdvTrackMult.cpp:760-777
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, s.scale}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma}, StoreArr<T>{np}))) return rc;
+    return SMADFT_OK;
+}
+
+template <typename T>
+int one_step(Ctx &c, bool keep_old)
+{
+    int rc;
+    switch (c.p.model) {
+    case SMADFT_MODEL_NOADV: rc = noadv_step<T>(c, keep_old); break;
+    case SMADFT_MODEL_ADV: rc = adv_step<T>(c); break;
+    default: rc = quasi_step<T>(c, c.steps + 1, keep_old); break;
+    }
+    return rc;
+}
+
+// psi of the current state into S_PSI (adv keeps only psihat between steps)
+template <typename T>
+int ensure_psi(Ctx &c)
+{
+    if (c.p.model == SMADFT_MODEL_ADV && !c.psi_current) {
+        int rc = refresh_psi<T>(c, c.f<T>(S_PSI));
+        if (rc) return rc;
+        c.psi_current = true;
+    }
+    return SMADFT_OK;
+}
+
+template <typename T>
+int step_diag_t(Ctx &c, smadft_diag *out)
+{
+    int rc;
+    // psi_old must hold psi at the start of the step
+    if ((rc = ensure_psi<T>(c))) return rc;
+    if (c.p.model == SMADFT_MODEL_ADV) {
+        if ((rc = adv_step<T>(c))) return rc;
+        // adv compares with the round-tripped psi of the step (adv/cosAdvTrackMult.cpp:961-963)
+        if ((rc = refresh_psi<T>(c, c.f<T>(S_PSI2)))) return rc;
+    } else {
+        if ((rc = one_step<T>(c, true))) return rc;
+    }
+    c.steps++;
+    double sums[4];
+    const T *nw = c.f<T>(S_PSI2), *od = c.f<T>(S_PSI);
+    if ((rc = reduce_l1<T>(c, nw, od, sums))) return rc;
+    double ms[2] = {0, 0};
+    if (c.p.model == SMADFT_MODEL_QUASI) {
+        if ((rc = reduce_mass_energy<T>(c, ms))) return rc;
+    }
+    std::swap(c.slot[S_PSI], c.slot[S_PSI2]);
+    c.psi_current = true;
+    out->l1 = sums[0] / (c.p.dt * sums[1]);
+    out->mean = sums[2] / (double)c.n;
+    out->nonfinite = (sums[3] != 0.0 || !std::isfinite(sums[1])) ? 1 : 0;
+    const double dx3 = c.dx * c.dx * c.dx;
+    out->mass = ms[0] * dx3;
+    out->energy = ms[1] * dx3;
+    out->steps = c.steps;
+    return out->nonfinite ? fail(c, SMADFT_ERR_NONFINITE, "psi is not finite") : SMADFT_OK;
+}
+
+template <typename T>
+int free_energy_t(Ctx &c, double *out)
+{
+    int rc;
+    if ((rc = ensure_psi<T>(c))) return rc;
+    Spec<T> s = make_spec<T>(c);
+    T *fp = c.f<T>(S_PSI2);
+    // f' = REDFT01^3(alpha (q0^2 - q^2) psihat)  (quasi/quasi.cpp:1121-1137)
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdDfd<T>{s, c.f<T>(S_PSIH)}, StoreArr<T>{fp}))) return rc;
+    double e;
+    if ((rc = reduce_energy<T>(c, c.f<T>(S_PSI), fp, &e))) return rc;
+    *out = e * c.dx * c.dx * c.dx;
+    return SMADFT_OK;
+}
+
+template <typename T>
+int set_psi_t(Ctx &c, const double *h)
+{
+    std::vector<T> tmp(c.n);
+    for (long long q = 0; q < c.n; q++) tmp[q] = T(h[q]);
+    SMADFT_CUDA(cudaMemcpyAsync(c.slot[S_PSI], tmp.data(), sizeof(T) * c.n, cudaMemcpyHostToDevice,
+                                c.stream));
+    int rc = pre_loop<T>(c);
+    if (rc) return rc;
+    SMADFT_CUDA(cudaStreamSynchronize(c.stream));
+    return SMADFT_OK;
+}
+
+template <typename T>
+int get_slot_t(Ctx &c, int slot, double *h)
+{
+    std::vector<T> tmp(c.n);
+    SMADFT_CUDA(cudaMemcpyAsync(tmp.data(), c.slot[slot], sizeof(T) * c.n, cudaMemcpyDeviceToHost,
+                                c.stream));
+    SMADFT_CUDA(cudaStreamSynchronize(c.stream));
+    for (long long q = 0; q < c.n; q++) h[q] = double(tmp[q]);
+    return SMADFT_OK;
+}
+
+template <typename T>
+int step_host_t(Ctx &c, double *host, int nsteps)
+{
+    if (!c.stage) SMADFT_CUDA(cudaMalloc(&c.stage, sizeof(double) * c.n));
+    SMADFT_CUDA(cudaMemcpyAsync(c.stage, host, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream));
+    Spec<T> s = make_spec<T>(c);
+    T *psi = c.f<T>(S_PSI);
+    int rc;
+    // psi from the host; psihat = scale REDFT10^3 psi (the reference's per-step planPsi)
+    if ((rc = convert<double, T>(c, c.stage, psi))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{c.f<T>(S_PSIH), s.scale}))) return rc;
+    c.psi_current = true;
+    for (int q = 0; q < nsteps; q++) {
+        if ((rc = one_step<T>(c, false))) return rc;
+        c.steps++;
+        c.psi_current = (c.p.model != SMADFT_MODEL_ADV);
+    }
+    if ((rc = ensure_psi<T>(c))) return rc;
+    if ((rc = convert<T, double>(c, psi, c.stage))) return rc;
+    SMADFT_CUDA(cudaMemcpyAsync(host, c.stage, sizeof(double) * c.n, cudaMemcpyDeviceToHost, c.stream));
+    SMADFT_CUDA(cudaStreamSynchronize(c.stream));
+    return SMADFT_OK;
+}
+
+template <typename T>
+int track_t(Ctx &c, int field, int axis, int mode, double hi, double lo, int *idx, double *pos)
+{
+    int rc;
+    if (field == SMADFT_FIELD_PSI && (rc = ensure_psi<T>(c))) return rc;
+    const T *f = c.f<T>(field == SMADFT_FIELD_RHO ? S_RHO : S_PSI);
+    if (!f) return fail(c, SMADFT_ERR_INVALID, "field not available for this model");
+    return track_columns<T>(c, f, axis, mode, hi, lo, idx, pos);
+}
+
+}  // namespace
+
+// ====================================================================== C ABI ==========
+extern "C" {
+
+int smadft_abi_version(void) { return SMADFT_ABI_VERSION; }
+
+const char *smadft_error_string(int code)
+{
+    switch (code) {
+    case SMADFT_OK: return "ok";
+    case SMADFT_ERR_INVALID: return "invalid argument";
+    case SMADFT_ERR_CUDA: return "CUDA error";
+    case SMADFT_ERR_NOMEM: return "out of memory";
+    case SMADFT_ERR_NONFINITE: return "non-finite field";
+    case SMADFT_ERR_TIMEOUT: return "device wait timed out";
+    case SMADFT_ERR_UNSUPPORTED: return "unsupported grid length";
+    case SMADFT_ERR_IO: return "checkpoint I/O error";
+    case SMADFT_ERR_STATE: return "call out of order";
+    case SMADFT_ERR_NODEVICE: return "no CUDA device";
+    default: return "unknown error";
+    }
+}
+
+void smadft_params_init(smadft_params *p, int model)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->model = model;
+    p->precision = SMADFT_FP64;
+    p->nx = p->ny = p->nz = 64;
+    p->nw = 8.0;
+    p->dt = (model == SMADFT_MODEL_NOADV) ? 0.05 : 0.02;
+    p->alpha = 1.0; p->beta = 2.0; p->gamma = 1.0; p->eps = -0.75; p->q0 = 1.0;
+    p->nu = 1.0;
+    p->rho0 = 1.0; p->kp = 0.0; p->amp = 1.34164;   // quasi/quasi.cpp:241-243
+    p->divv_switch = 200;                            // quasi/quasi.cpp:206
+    p->loaded = 0;
+    p->device = 0;
+}
+
+int smadft_params_check(const smadft_params *p)
+{
+    if (!p) return SMADFT_ERR_INVALID;
+    if (p->model < 0 || p->model > 2) return SMADFT_ERR_INVALID;
+    if (p->precision != SMADFT_FP64 && p->precision != SMADFT_FP32) return SMADFT_ERR_INVALID;
+    if (p->nx < 4 || p->ny < 4 || p->nz < 4) return SMADFT_ERR_INVALID;
+    if (p->nx > 1024 || p->ny > 1024 || p->nz > 1024) return SMADFT_ERR_UNSUPPORTED;
+    if (!factor_ok(p->nx) || !factor_ok(p->ny) || !factor_ok(p->nz)) return SMADFT_ERR_UNSUPPORTED;
+    if (!(p->nw > 0) || !(p->dt > 0) || !(p->q0 > 0)) return SMADFT_ERR_INVALID;
+    if (p->model != SMADFT_MODEL_NOADV && !(p->nu > 0)) return SMADFT_ERR_INVALID;
+    if (p->model == SMADFT_MODEL_QUASI && !(p->rho0 > 0)) return SMADFT_ERR_INVALID;
+    return SMADFT_OK;
+}
+
+int smadft_create(const smadft_params *p, smadft_ctx **out)
+{
+    if (!out) return SMADFT_ERR_INVALID;
+    *out = nullptr;
+    int rc = smadft_params_check(p);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return SMADFT_ERR_NODEVICE;
+    }
+    if (p->device < 0 || p->device >= ndev) return SMADFT_ERR_INVALID;
+    smadft_ctx *h = new (std::nothrow) smadft_ctx;
+    if (!h) return SMADFT_ERR_NOMEM;
+    Ctx &c = h->c;
+    c.p = *p;
+    c.f32 = p->precision == SMADFT_FP32;
+    c.esize = c.f32 ? 4 : 8;
+    c.dev = p->device;
+    c.g.nx = p->nx; c.g.ny = p->ny; c.g.nz = p->nz;
+    c.g.nyz = (long long)p->ny * p->nz;
+    c.n = (long long)p->nx * p->ny * p->nz;
+    // box: no-adv/cosNoAdvTrackSing.cpp:160-172
+    c.Lx = p->nx * 2.0 * M_PI / (p->q0 * p->nw);
+    c.Ly = p->ny * 2.0 * M_PI / (p->q0 * p->nw);
+    c.Lz = p->nz * 2.0 * M_PI / (p->q0 * p->nw);
+    c.dx = c.Lx / p->nx; c.dy = c.Ly / p->ny; c.dz = c.Lz / p->nz;
+    c.scale = 0.125 / ((double)p->nx * p->ny * p->nz);
+    auto bail = [&](int code) { smadft_destroy(h); return code; };
+    if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+    for (int s : slots_for(p->model)) {
+        if (cudaMalloc(&c.slot[s], c.esize * c.n) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
+        if (cudaMemset(c.slot[s], 0, c.esize * c.n) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+    }
+    for (int n : {p->nx, p->ny, p->nz}) {
+        rc = c.f32 ? upload_plan<float>(c, n) : upload_plan<double>(c, n);
+        if (rc) return bail(rc);
+    }
+    rc = c.f32 ? upload_tables<float>(c) : upload_tables<double>(c);
+    if (rc) return bail(rc);
+    if ((rc = reduce_init(c))) return bail(rc);
+    *out = h;
+    return SMADFT_OK;
+}
+
+int smadft_destroy(smadft_ctx *h)
+{
+    if (!h) return SMADFT_OK;
+    Ctx &c = h->c;
+    cudaSetDevice(c.dev);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    for (int s = 0; s < S_COUNT; s++)
+        if (c.slot[s]) cudaFree(c.slot[s]);
+    for (auto &kv : c.plans) { cudaFree(kv.second.w); cudaFree(kv.second.h); }
+    if (c.tables) cudaFree(c.tables);
+    if (c.red) cudaFree(c.red);
+    if (c.red_out) cudaFree(c.red_out);
+    if (c.stage) cudaFree(c.stage);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    cudaGetLastError();
+    delete h;
+    return SMADFT_OK;
+}
+
+const char *smadft_last_error(const smadft_ctx *h)
+{
+    if (!h) return "null context";
+    return h->c.err.c_str();
+}
+
+int smadft_set_psi(smadft_ctx *h, const double *host, size_t n)
+{
+    if (!h || !host) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if ((long long)n != c.n) return fail(c, SMADFT_ERR_INVALID, "size mismatch");
+    cudaSetDevice(c.dev);
+    for (int s = 0; s < S_COUNT; s++)
+        if (c.slot[s] && s != S_PSI) {
+            if (cudaMemsetAsync(c.slot[s], 0, c.esize * c.n, c.stream) != cudaSuccess)
+                return fail(c, SMADFT_ERR_CUDA, "memset");
+        }
+    int rc = c.f32 ? set_psi_t<float>(c, host) : set_psi_t<double>(c, host);
+    if (rc) return rc;
+    c.steps = 0;
+    c.have_psi = true;
+    c.psi_current = true;
+    return SMADFT_OK;
+}
+
+int smadft_get_psi(smadft_ctx *h, double *host, size_t n)
+{
+    return smadft_get_field(h, SMADFT_FIELD_PSI, host, n);
+}
+
+int smadft_get_field(smadft_ctx *h, int field, double *host, size_t n)
+{
+    if (!h || !host) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if ((long long)n != c.n) return fail(c, SMADFT_ERR_INVALID, "size mismatch");
+    if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
+    cudaSetDevice(c.dev);
+    int slot;
+    switch (field) {
+    case SMADFT_FIELD_PSI: slot = S_PSI; break;
+    case SMADFT_FIELD_PSIHAT: slot = S_PSIH; break;
+    case SMADFT_FIELD_VX: slot = S_VX; break;
+    case SMADFT_FIELD_VY: slot = S_VY; break;
+    case SMADFT_FIELD_VZ: slot = S_VZ; break;
+    case SMADFT_FIELD_GX: slot = S_GX; break;
+    case SMADFT_FIELD_GY: slot = S_GY; break;
+    case SMADFT_FIELD_GZ: slot = S_GZ; break;
+    case SMADFT_FIELD_RHO: slot = S_RHO; break;
+    case SMADFT_FIELD_P: slot = S_P; break;
+    case SMADFT_FIELD_DIVV: slot = S_DIVV; break;
+    case SMADFT_FIELD_MU: slot = S_MU; break;
+    case SMADFT_FIELD_ENERGY: slot = S_EN; break;
+    case SMADFT_FIELD_NHAT: slot = S_NP; break;
+    default: return fail(c, SMADFT_ERR_INVALID, "unknown field");
+    }
+    if (!c.slot[slot]) return fail(c, SMADFT_ERR_INVALID, "field not available for this model");
+    int rc;
+    if (slot == S_PSI) {
+        rc = c.f32 ? ensure_psi<float>(c) : ensure_psi<double>(c);
+        if (rc) return rc;
+    }
+    return c.f32 ? get_slot_t<float>(c, slot, host) : get_slot_t<double>(c, slot, host);
+}
+
+int smadft_step(smadft_ctx *h, int nsteps)
+{
+    if (!h || nsteps < 0) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
+    cudaSetDevice(c.dev);
+    for (int s = 0; s < nsteps; s++) {
+        int rc = c.f32 ? one_step<float>(c, false) : one_step<double>(c, false);
+        if (rc) return rc;
+        c.steps++;
+        c.psi_current = (c.p.model != SMADFT_MODEL_ADV);
+    }
+    return SMADFT_OK;
+}
+
+int smadft_step_diag(smadft_ctx *h, smadft_diag *out)
+{
+    if (!h || !out) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
+    cudaSetDevice(c.dev);
+    std::memset(out, 0, sizeof(*out));
+    return c.f32 ? step_diag_t<float>(c, out) : step_diag_t<double>(c, out);
+}
+
+int smadft_sync(smadft_ctx *h)
+{
+    if (!h) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    cudaSetDevice(c.dev);
+    SMADFT_CUDA(cudaStreamSynchronize(c.stream));
+    return SMADFT_OK;
+}
+
+int smadft_track(smadft_ctx *h, int field, int axis, int mode, double hi, double lo, int *idx,
+                 double *pos)
+{
+    if (!h || !idx || !pos || axis < 0 || axis > 2 || mode < 0 || mode > 2) return SMADFT_ERR_INVALID;
+    if (field != SMADFT_FIELD_PSI && field != SMADFT_FIELD_RHO) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
+    cudaSetDevice(c.dev);
+    return c.f32 ? track_t<float>(c, field, axis, mode, hi, lo, idx, pos)
+                 : track_t<double>(c, field, axis, mode, hi, lo, idx, pos);
+}
+
+int smadft_free_energy(smadft_ctx *h, double *out)
+{
+    if (!h || !out) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
+    cudaSetDevice(c.dev);
+    return c.f32 ? free_energy_t<float>(c, out) : free_energy_t<double>(c, out);
+}
+
+int smadft_step_host(smadft_ctx *h, double *host, size_t n, int nsteps)
+{
+    if (!h || !host || nsteps < 0) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if ((long long)n != c.n) return fail(c, SMADFT_ERR_INVALID, "size mismatch");
+    if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
+    cudaSetDevice(c.dev);
+    return c.f32 ? step_host_t<float>(c, host, nsteps) : step_host_t<double>(c, host, nsteps);
+}
+
+int smadft_get_stream(smadft_ctx *h, void **stream)
+{
+    if (!h || !stream) return SMADFT_ERR_INVALID;
+    *stream = (void *)h->c.stream;
+    return SMADFT_OK;
+}
+
+int smadft_launch_count(const smadft_ctx *h, long long *count)
+{
+    if (!h || !count) return SMADFT_ERR_INVALID;
+    *count = h->c.launches;
+    return SMADFT_OK;
+}
+
+int smadft_r2r_pass_device(smadft_ctx *h, const void *in, void *out, int axis, int kind)
+{
+    if (!h || !in || !out || axis < 0 || axis > 2 || kind < 0 || kind > 3) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    cudaSetDevice(c.dev);
+    if (c.f32)
+        return launch_pass<float>(c, axis, kind, LoadArr<float>{(const float *)in}, StoreArr<float>{(float *)out});
+    return launch_pass<double>(c, axis, kind, LoadArr<double>{(const double *)in}, StoreArr<double>{(double *)out});
+}
+
+int smadft_r2r3d_device(smadft_ctx *h, const void *in, void *out, int kx, int ky, int kz)
+{
+    if (!h || !in || !out) return SMADFT_ERR_INVALID;
+    for (int k : {kx, ky, kz})
+        if (k < 0 || k > 3) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    cudaSetDevice(c.dev);
+    if (c.f32)
+        return r2r3d<float>(c, kx, ky, kz, LoadArr<float>{(const float *)in}, StoreArr<float>{(float *)out});
+    return r2r3d<double>(c, kx, ky, kz, LoadArr<double>{(const double *)in}, StoreArr<double>{(double *)out});
+}
+
+}  // extern "C"
+
+#include "checkpoint.inc"

@@ -1,0 +1,207 @@
+"""GPU time stepping against the oracle and the golden vectors (through the C ABI).
+
+Bars: the FP64 GPU path matches the reference within 1e-10 relative;
+FP32 results state their relative L2 error against FP64 (asserted loosely here).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import smadft
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+MODEL = {"noadv": smadft.NOADV, "bump": smadft.NOADV, "adv": smadft.ADV, "quasi": smadft.QUASI}
+OMODEL = {smadft.NOADV: oracle.NOADV, smadft.ADV: oracle.ADV, smadft.QUASI: oracle.QUASI}
+GFIELD = {"psi": "psi", "nq": "nhat", "vx": "vx", "vy": "vy", "vz": "vz", "gx": "gx", "gy": "gy",
+          "gz": "gz", "rho": "rho", "p": "p", "mu": "mu", "energy": "energy", "psiq": "psihat"}
+
+
+def rel_max(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def solver_for(which, shape, params, precision=smadft.FP64):
+    kw = dict(params)
+    divv = int(kw.pop("divv", 200))
+    p = smadft.params(MODEL[which], shape, precision=precision, divv_switch=divv, **kw)
+    return smadft.Solver(p)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_fp64_matches_golden(path):
+    d = np.load(path)
+    which = str(d["which"])
+    params = dict(zip([str(k) for k in d["params_keys"]], [float(v) for v in d["params_vals"]]))
+    shape = tuple(int(s) for s in d["shape"])
+    steps = int(d["steps"])
+    stepL1 = 50 if which == "quasi" else 100
+    with solver_for(which, shape, params) as s:
+        s.set_psi(d["psi0"])
+        l1, mass, energy = [], [], []
+        done = 0
+        while done < steps:
+            nxt = min(steps, (done // stepL1 + 1) * stepL1)
+            if nxt - done > 1:
+                s.step(nxt - done - 1)
+            if nxt % stepL1 == 0:
+                dg = s.step_diag()
+                l1.append(dg["l1"]); mass.append(dg["mass"]); energy.append(dg["energy"])
+            else:
+                s.step(1)
+            done = nxt
+        for key in d.files:
+            if key.startswith("f_"):
+                got = s.get(GFIELD[key[2:]])
+                assert rel_max(got, d[key]) <= 1e-10, key
+        if "t_L1" in d.files:
+            assert np.allclose(l1, d["t_L1"], rtol=1e-10, atol=0)
+        if "t_mass" in d.files:
+            assert np.allclose(mass, d["t_mass"], rtol=1e-10, atol=0)
+            assert np.allclose(energy, d["t_energy"], rtol=1e-10, atol=0)
+        if "t_surfPsi" in d.files:
+            idx, pos = s.track(axis=2, mode=smadft.TRACK_BUMP, hi=0.6, lo=0.1)
+            idx = idx.reshape(-1)
+            found = idx >= 0
+            assert found.sum() > idx.size // 4
+            assert np.array_equal(idx[found].astype(float), d["t_surfPsi"][found])
+
+
+def config1_ic(shape):
+    p = smadft.params(smadft.NOADV, shape)
+    return smadft.ic_interface(p, A=0.5, bump=0.0, noise=1e-3, seed=20240601)
+
+
+def test_config1_noadv_64cubed_1000_steps_fp64():
+    """Config 1: 64^3 noadv FP64, dx = lambda0/8, dt = 0.05, 1000 steps: rel L2 <= 1e-10."""
+    shape = (64, 64, 64)
+    psi0 = config1_ic(shape)
+    o = oracle.Oracle(oracle.NOADV, shape, nw=8, dt=0.05, eps=-0.75)
+    o.set_psi(psi0)
+    o.step(1000)
+    with smadft.Solver(smadft.params(smadft.NOADV, shape)) as s:
+        s.set_psi(psi0)
+        s.step(999)
+        dg = s.step_diag()
+        got = s.get("psi")
+    ref = o.get()
+    assert rel_l2(got, ref) <= 1e-10
+    assert abs(dg["l1"] - o.diag()["l1"]) <= 1e-10 * abs(o.diag()["l1"])
+
+
+@pytest.mark.parametrize("model,shape,steps,kw", [
+    (smadft.NOADV, (32, 24, 40), 50, dict(dt=0.05)),
+    (smadft.ADV, (32, 24, 40), 30, dict(dt=0.02)),
+    (smadft.QUASI, (24, 20, 32), 30, dict(dt=0.002, kp=0.3755, divv_switch=10)),
+])
+def test_fp64_matches_oracle_fields(model, shape, steps, kw):
+    p = smadft.params(model, shape, **kw)
+    psi0 = smadft.ic_conics(p, A=1.3, count=2, rmin=1.0, rmax=2.0, noise=1e-3, seed=3)
+    okw = dict(nw=p.nw, dt=p.dt, eps=p.eps, nu=p.nu, kp=p.kp, rho0=p.rho0, divv_switch=p.divv_switch)
+    o = oracle.Oracle(OMODEL[model], shape, **okw)
+    o.set_psi(psi0)
+    o.step(steps)
+    with smadft.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(steps)
+        assert rel_max(s.get("psi"), o.get(oracle.F_PSI)) <= 1e-10
+        if model != smadft.NOADV:
+            for f, of in [("vx", oracle.F_VX), ("vy", oracle.F_VY), ("vz", oracle.F_VZ), ("gz", oracle.F_GZ)]:
+                assert rel_max(s.get(f), o.get(of)) <= 1e-9, f
+        if model == smadft.QUASI:
+            for f, of in [("rho", oracle.F_RHO), ("p", oracle.F_P), ("mu", oracle.F_MU)]:
+                assert rel_max(s.get(f), o.get(of)) <= 1e-9, f
+
+
+@pytest.mark.parametrize("model,steps,tol", [(smadft.NOADV, 200, 1e-5), (smadft.ADV, 100, 1e-5)])
+def test_fp32_error_vs_fp64(model, steps, tol):
+    shape = (48, 40, 64)
+    p64 = smadft.params(model, shape)
+    psi0 = smadft.ic_conics(p64, A=1.3, count=3, rmin=1.0, rmax=2.0, noise=1e-3, seed=9)
+    out = {}
+    for prec in (smadft.FP64, smadft.FP32):
+        with smadft.Solver(smadft.params(model, shape, precision=prec)) as s:
+            s.set_psi(psi0)
+            s.step(steps)
+            out[prec] = s.get("psi")
+    err = rel_l2(out[smadft.FP32], out[smadft.FP64])
+    print(f"model {model} fp32 rel L2 vs fp64 after {steps} steps: {err:.3e}")
+    assert err <= tol
+
+
+def test_free_energy_matches_oracle():
+    shape = (32, 24, 40)
+    p = smadft.params(smadft.NOADV, shape)
+    psi0 = smadft.ic_conics(p, A=1.3, count=2, rmin=1.0, rmax=2.0, noise=1e-3, seed=4)
+    o = oracle.Oracle(oracle.NOADV, shape)
+    o.set_psi(psi0)
+    o.step(10)
+    with smadft.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(10)
+        e = s.free_energy()
+    assert abs(e - o.free_energy()) <= 1e-10 * abs(o.free_energy())
+
+
+@pytest.mark.parametrize("axis,mode,hi,lo", [(2, 0, 0.7, 0.0), (2, 1, 0.6, 0.1), (0, 1, 0.6, 0.1)])
+def test_tracker_matches_oracle(axis, mode, hi, lo):
+    shape = (32, 24, 40)
+    p = smadft.params(smadft.NOADV, shape, eps=-0.7)
+    psi0 = smadft.ic_interface(p, A=1.328, bump=4.0, noise=1e-3, seed=8)
+    o = oracle.Oracle(oracle.NOADV, shape, eps=-0.7)
+    o.set_psi(psi0)
+    o.step(20)
+    with smadft.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(20)
+        idx, pos = s.track(axis=axis, mode=mode, hi=hi, lo=lo)
+    oi, op = o.track(axis=axis, mode=mode, hi=hi, lo=lo)
+    assert np.array_equal(idx, oi)
+    m = np.isfinite(op)
+    assert np.array_equal(np.isfinite(pos), m)
+    assert np.allclose(pos[m], op[m], rtol=0, atol=1e-9)
+
+
+def test_checkpoint_resume_is_exact(tmp_path):
+    shape = (24, 20, 32)
+    for model in (smadft.NOADV, smadft.ADV, smadft.QUASI):
+        p = smadft.params(model, shape, dt=0.002 if model == smadft.QUASI else 0.02, kp=0.3, divv_switch=3)
+        psi0 = smadft.ic_conics(p, A=1.3, count=2, rmin=1.0, rmax=2.0, seed=1)
+        ck = str(tmp_path / f"m{model}.ck")
+        with smadft.Solver(p) as a:
+            a.set_psi(psi0)
+            a.step(5)
+            a.save(ck)
+            a.step(5)
+            want = a.get("psi")
+        with smadft.Solver(p) as b:
+            b.load(ck)
+            b.step(5)
+            got = b.get("psi")
+        assert np.array_equal(got, want), model
+
+
+def test_nonfinite_is_reported():
+    shape = (16, 16, 16)
+    p = smadft.params(smadft.NOADV, shape)
+    psi0 = np.zeros(shape)
+    psi0[3, 4, 5] = np.nan          # planted on the host; arithmetic only, no memory fault
+    with smadft.Solver(p) as s:
+        s.set_psi(psi0)
+        d = s.step_diag()
+    assert d["rc"] == -4 and d["nonfinite"] == 1
+
+
+def test_step_before_psi_is_state_error():
+    with smadft.Solver(smadft.params(smadft.NOADV, (16, 16, 16))) as s:
+        with pytest.raises(smadft.SmadftError) as e:
+            s.step(1)
+        assert e.value.code == -8
