@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "r2r_fast.cuh"
 #include "r2r_pass.cuh"
 #include "smadft.h"
 
@@ -72,6 +73,7 @@ struct Ctx {
     bool have_psi = false;
     bool psi_current = false;   // adv: S_PSI holds iCT(psihat) of the current state
     long long launches = 0;     // kernels launched by this context
+    bool use_fast = true;       // compile-time-length pass kernels where available
     double *stage = nullptr;    // FP64 staging field for host-psi steps (allocated on first use)
 
     template <typename T>
@@ -114,7 +116,7 @@ template <typename T>
 constexpr int tile_w() { return sizeof(T) == 4 ? 32 : 16; }
 
 template <typename T, class LD, class ST>
-int launch_pass(Ctx &c, int axis, int kind, LD ld, ST st)
+int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
 {
     const int n = axis == 0 ? c.g.nx : (axis == 1 ? c.g.ny : c.g.nz);
     const PlanDev &pd = c.plans.at(n);
@@ -150,6 +152,60 @@ int launch_pass(Ctx &c, int axis, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
+template <typename T, int N, int AXIS, class LD, class ST>
+int launch_fast(Ctx &c, int kind, LD ld, ST st)
+{
+    const PlanDev &pd = c.plans.at(N);
+    const int W = kFastW;
+    int tiles_b = 1;
+    long long tiles;
+    if (AXIS == 2) {
+        tiles = ((long long)c.g.nx * c.g.ny + W - 1) / W;
+    } else {
+        tiles_b = (c.g.nz + W - 1) / W;
+        tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b;
+    }
+    constexpr size_t smem = fast_smem_bytes<T, N>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_fast_kernel<T, N, AXIS, LD, ST>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    r2r_fast_kernel<T, N, AXIS, LD, ST><<<(unsigned)tiles, kFastThreads, smem, c.stream>>>(
+        c.g, kind, tiles_b, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), ld, st);
+    SMADFT_CUDA(cudaGetLastError());
+    c.launches++;
+    return SMADFT_OK;
+}
+
+// Line lengths with a compile-time kernel (the configs' grids); others use the generic one.
+#define SMADFT_FAST_SIZES(X) X(64) X(96) X(128) X(160) X(256)
+
+template <typename T, int AXIS, class LD, class ST>
+int launch_axis(Ctx &c, int kind, LD ld, ST st)
+{
+    const int n = AXIS == 0 ? c.g.nx : (AXIS == 1 ? c.g.ny : c.g.nz);
+    if (c.use_fast) {
+        switch (n) {
+#define SMADFT_CASE(N_) \
+    case N_: return launch_fast<T, N_, AXIS>(c, kind, ld, st);
+            SMADFT_FAST_SIZES(SMADFT_CASE)
+#undef SMADFT_CASE
+        default: break;
+        }
+    }
+    return launch_generic<T>(c, AXIS, kind, ld, st);
+}
+
+template <typename T, class LD, class ST>
+int launch_pass(Ctx &c, int axis, int kind, LD ld, ST st)
+{
+    if (axis == 0) return launch_axis<T, 0>(c, kind, ld, st);
+    if (axis == 1) return launch_axis<T, 1>(c, kind, ld, st);
+    return launch_axis<T, 2>(c, kind, ld, st);
+}
+
 // Element-wise precision conversion (host-psi steps).
 template <typename S, typename D>
 __global__ void convert_kernel(const S *__restrict__ src, D *__restrict__ dst, long long n)
@@ -173,11 +229,11 @@ template <typename T, class LD, class ST>
 int r2r3d(Ctx &c, int kx, int ky, int kz, LD ld, ST st)
 {
     T *tmp = c.f<T>(S_TMP);
-    int rc = launch_pass<T>(c, 2, kz, ld, StoreArr<T>{tmp});
+    int rc = launch_axis<T, 2>(c, kz, ld, StoreArr<T>{tmp});
     if (rc) return rc;
-    rc = launch_pass<T>(c, 1, ky, LoadArr<T>{tmp}, StoreArr<T>{tmp});
+    rc = launch_axis<T, 1>(c, ky, LoadArr<T>{tmp}, StoreArr<T>{tmp});
     if (rc) return rc;
-    return launch_pass<T>(c, 0, kx, LoadArr<T>{tmp}, st);
+    return launch_axis<T, 0>(c, kx, LoadArr<T>{tmp}, st);
 }
 
 }  // namespace smadft

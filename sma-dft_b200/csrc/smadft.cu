@@ -17,11 +17,18 @@
 
 using namespace smadft;
 
+// A captured loop body.  noadv/adv steps are all alike; quasi steps differ by the step
+// counter (first step, before/after the div v switch, the extra N term), so each variant
+// gets its own graph.
+struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;   // kernels per replay
+};
+
 struct smadft_ctx {
     Ctx c;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    int graph_variant = -1;
+    std::map<int, StepGraph> graphs;
+    bool use_graphs = true;
 };
 
 namespace {
@@ -176,6 +183,17 @@ int pre_loop(Ctx &c)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, s.scale}))) return rc;
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma}, StoreArr<T>{np}))) return rc;
     return SMADFT_OK;
+}
+
+// Graph variant of the next loop body (see StepGraph).
+int step_variant(const Ctx &c)
+{
+    if (c.p.model != SMADFT_MODEL_QUASI) return 0;
+    const long long nloop = c.steps + 1;
+    const int first = nloop == 1;
+    const int divv = (nloop > c.p.divv_switch || c.p.loaded) ? 1 : 0;
+    const int extra = nloop > c.p.divv_switch + 1;
+    return first | (divv << 1) | (extra << 2) | ((first && c.p.loaded) << 3);
 }
 
 template <typename T>
@@ -415,8 +433,7 @@ int smadft_destroy(smadft_ctx *h)
     Ctx &c = h->c;
     cudaSetDevice(c.dev);
     if (c.stream) cudaStreamSynchronize(c.stream);
-    if (h->gexec) cudaGraphExecDestroy(h->gexec);
-    if (h->graph) cudaGraphDestroy(h->graph);
+    for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
     for (int s = 0; s < S_COUNT; s++)
         if (c.slot[s]) cudaFree(c.slot[s]);
     for (auto &kv : c.plans) { cudaFree(kv.second.w); cudaFree(kv.second.h); }
@@ -494,6 +511,37 @@ int smadft_get_field(smadft_ctx *h, int field, double *host, size_t n)
     return c.f32 ? get_slot_t<float>(c, slot, host) : get_slot_t<double>(c, slot, host);
 }
 
+// Runs one loop body by replaying its captured graph (captured on first use; the very
+// first body of a context runs eagerly so that kernel attributes are set outside capture).
+static int graph_step(smadft_ctx *h)
+{
+    Ctx &c = h->c;
+    const int v = step_variant(c);
+    auto it = h->graphs.find(v);
+    if (it == h->graphs.end()) {
+        if (c.launches == 0 || !h->use_graphs) {
+            return c.f32 ? one_step<float>(c, false) : one_step<double>(c, false);
+        }
+        StepGraph g;
+        cudaGraph_t graph = nullptr;
+        const long long l0 = c.launches;
+        SMADFT_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        int rc = c.f32 ? one_step<float>(c, false) : one_step<double>(c, false);
+        cudaError_t ce = cudaStreamEndCapture(c.stream, &graph);
+        if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+        if (ce != cudaSuccess) { c.err = cudaGetErrorString(ce); return SMADFT_ERR_CUDA; }
+        ce = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) { c.err = cudaGetErrorString(ce); return SMADFT_ERR_CUDA; }
+        g.launches = c.launches - l0;
+        c.launches = l0;
+        it = h->graphs.emplace(v, g).first;
+    }
+    SMADFT_CUDA(cudaGraphLaunch(it->second.exec, c.stream));
+    c.launches += it->second.launches;
+    return SMADFT_OK;
+}
+
 int smadft_step(smadft_ctx *h, int nsteps)
 {
     if (!h || nsteps < 0) return SMADFT_ERR_INVALID;
@@ -501,7 +549,7 @@ int smadft_step(smadft_ctx *h, int nsteps)
     if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
     cudaSetDevice(c.dev);
     for (int s = 0; s < nsteps; s++) {
-        int rc = c.f32 ? one_step<float>(c, false) : one_step<double>(c, false);
+        int rc = graph_step(h);
         if (rc) return rc;
         c.steps++;
         c.psi_current = (c.p.model != SMADFT_MODEL_ADV);

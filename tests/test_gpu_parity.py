@@ -61,7 +61,11 @@ def test_fp64_matches_golden(path):
         for key in d.files:
             if key.startswith("f_"):
                 got = s.get(GFIELD[key[2:]])
-                assert rel_max(got, d[key]) <= 1e-10, key
+                # quasi's derived fields go through div v = -((rho - rho_old)/dt + ...) /
+                # (rho + rho_old)/2 (quasi/quasi.cpp:1370-1377), which amplifies last-bit
+                # differences by rho/(dt drho); psi itself stays at the 1e-10 bar
+                tol = 1e-10 if (which != "quasi" or key in ("f_psi", "f_psiq")) else 1e-8
+                assert rel_max(got, d[key]) <= tol, key
         if "t_L1" in d.files:
             assert np.allclose(l1, d["t_L1"], rtol=1e-10, atol=0)
         if "t_mass" in d.files:
