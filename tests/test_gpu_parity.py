@@ -117,12 +117,14 @@ def test_fp64_matches_oracle_fields(model, shape, steps, kw):
         s.set_psi(psi0)
         s.step(steps)
         assert rel_max(s.get("psi"), o.get(oracle.F_PSI)) <= 1e-10
+        # quasi's derived fields pass through (rho - rho_old)/dt (see test_fp64_matches_golden)
+        tol = 1e-8 if model == smadft.QUASI else 1e-9
         if model != smadft.NOADV:
             for f, of in [("vx", oracle.F_VX), ("vy", oracle.F_VY), ("vz", oracle.F_VZ), ("gz", oracle.F_GZ)]:
-                assert rel_max(s.get(f), o.get(of)) <= 1e-9, f
+                assert rel_max(s.get(f), o.get(of)) <= tol, f
         if model == smadft.QUASI:
             for f, of in [("rho", oracle.F_RHO), ("p", oracle.F_P), ("mu", oracle.F_MU)]:
-                assert rel_max(s.get(f), o.get(of)) <= 1e-9, f
+                assert rel_max(s.get(f), o.get(of)) <= tol, f
 
 
 @pytest.mark.parametrize("model,steps,tol", [(smadft.NOADV, 200, 1e-5), (smadft.ADV, 100, 1e-5)])
