@@ -247,35 +247,62 @@ __device__ __forceinline__ ElemPos tile_elem(const Geom &g, const TileBase &tb, 
 constexpr int kFastW = 32;        // real lines per tile
 constexpr int kFastThreads = 256;
 
+// largest divisor of `per` not above 8
+constexpr int batch_size(int per)
+{
+    for (int b = 8; b > 1; b--)
+        if (per % b == 0) return b;
+    return 1;
+}
+
 template <typename T, int N>
-constexpr size_t fast_smem_bytes() { return (size_t)(kFastW / 2) * PlanInfo<N>::LD * sizeof(cpx<T>); }
+constexpr size_t fast_smem_bytes() { return ((size_t)(kFastW / 2) * PlanInfo<N>::LD + 2 * N) * sizeof(cpx<T>); }
 
 template <typename T, int N, int AXIS, class LD, class ST>
-__global__ void __launch_bounds__(kFastThreads) r2r_fast_kernel(Geom g, int kind, int tiles_b,
-                                                                const cpx<T> *__restrict__ wt,
-                                                                const cpx<T> *__restrict__ ht, LD ld, ST st)
+__global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int kind, int tiles_b,
+                                                                   const cpx<T> *__restrict__ wt_g,
+                                                                   const cpx<T> *__restrict__ ht_g, LD ld, ST st)
 {
     using PI = PlanInfo<N>;
     constexpr int W = kFastW, NL = W / 2;
+    constexpr int PER = N * W / kFastThreads;     // tile elements per thread
+    constexpr int BATCH = batch_size(PER);        // loads in flight per thread
+    static_assert(PER % BATCH == 0, "tile must split evenly");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T> *buf = reinterpret_cast<cpx<T> *>(smem_raw);
+    cpx<T> *wt = buf + NL * PI::LD;               // FFT twiddles W_N^m
+    cpx<T> *ht = wt + N;                          // Makhoul twiddles exp(i pi k / 2N)
     T *rb = reinterpret_cast<T *>(smem_raw);
     const TileBase tb = tile_base<AXIS>(g, W, tiles_b);
     const bool fwd = (kind == K_DCT2 || kind == K_DST2);
+    for (int m = threadIdx.x; m < N; m += kFastThreads) {
+        wt[m] = wt_g[m];
+        ht[m] = ht_g[m];
+    }
 
-    // ---- global -> shared, input permutation per kind
-    for (int e = threadIdx.x; e < N * W; e += kFastThreads) {
-        int t, w;
-        if (AXIS == 2) { t = e % N; w = e / N; }
-        else { w = e % W; t = e / W; }
-        const ElemPos p = tile_elem<AXIS>(g, tb, t, w);
-        T v = p.valid ? ld(p.idx, p.i, p.j, p.k) : T(0);
-        int pos;
-        if (kind == K_DCT2) pos = makhoul_pos(t, N);
-        else if (kind == K_DST2) { pos = makhoul_pos(t, N); if (t & 1) v = -v; }
-        else if (kind == K_DCT3) pos = t;
-        else pos = N - 1 - t;
-        rb[2 * ((w >> 1) * PI::LD + PI::phys(pos)) + (w & 1)] = v;
+    // ---- global -> shared, input permutation per kind; BATCH independent loads per thread
+#pragma unroll 1
+    for (int e0 = 0; e0 < PER; e0 += BATCH) {
+        T vals[BATCH];
+        int spos[BATCH];
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) {
+            const int e = (e0 + b) * kFastThreads + threadIdx.x;
+            int t, w;
+            if (AXIS == 2) { t = e % N; w = e / N; }
+            else { w = e % W; t = e / W; }
+            const ElemPos p = tile_elem<AXIS>(g, tb, t, w);
+            T v = p.valid ? ld(p.idx, p.i, p.j, p.k) : T(0);
+            int pos;
+            if (kind == K_DCT2) pos = makhoul_pos(t, N);
+            else if (kind == K_DST2) { pos = makhoul_pos(t, N); if (t & 1) v = -v; }
+            else if (kind == K_DCT3) pos = t;
+            else pos = N - 1 - t;
+            vals[b] = v;
+            spos[b] = 2 * ((w >> 1) * PI::LD + PI::phys(pos)) + (w & 1);
+        }
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) rb[spos[b]] = vals[b];
     }
     __syncthreads();
 

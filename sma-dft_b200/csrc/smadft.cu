@@ -241,7 +241,8 @@ int step_diag_t(Ctx &c, smadft_diag *out)
     if (c.p.model == SMADFT_MODEL_QUASI) {
         if ((rc = reduce_mass_energy<T>(c, ms))) return rc;
     }
-    std::swap(c.slot[S_PSI], c.slot[S_PSI2]);
+    // psi_new -> S_PSI by copy: captured step graphs hold the slot pointers
+    SMADFT_CUDA(cudaMemcpyAsync(c.slot[S_PSI], c.slot[S_PSI2], c.esize * c.n, cudaMemcpyDeviceToDevice, c.stream));
     c.psi_current = true;
     out->l1 = sums[0] / (c.p.dt * sums[1]);
     out->mean = sums[2] / (double)c.n;
