@@ -180,6 +180,7 @@ def pass_roofline(torch, smadft, peak):
     with smadft.Solver(p) as s:
         x = torch.randn((N, N, N), device="cuda", dtype=torch.float32)
         y = torch.empty_like(x)
+        torch.cuda.synchronize()
         stream = torch.cuda.ExternalStream(s.stream)
         out = {}
         for axis, name in ((2, "z"), (1, "y"), (0, "x")):
@@ -311,13 +312,49 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def run_kernel_only(args):
+    """A few launches of one kernel family for profiling (ncu): no timing, no JSON.
+
+    pass-z | pass-y | pass-x: one plain DCT-II axis pass on a 256^3 field (2 fields held).
+    step: loop bodies of the adv model (all its kernels).
+    """
+    import torch
+    import smadft
+    prec = smadft.FP64 if args.precision == "fp64" else smadft.FP32
+    n = args.shape
+    p = smadft.params(smadft.ADV, (n, n, n), precision=prec, **CFG)
+    with smadft.Solver(p) as s:
+        if args.kernel_only.startswith("pass"):
+            dt = torch.float32 if prec == smadft.FP32 else torch.float64
+            x = torch.randn((n, n, n), device="cuda", dtype=dt)
+            y = torch.empty_like(x)
+            torch.cuda.synchronize()
+            axis = {"pass-z": 2, "pass-y": 1, "pass-x": 0}[args.kernel_only]
+            for _ in range(args.reps):
+                s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, 0)
+        else:
+            p2 = smadft.params(smadft.ADV, (n, n, n), **CFG)
+            s.set_psi(smadft.ic_conics(p2, A=1.328, count=4, rmin=3.0, rmax=6.0, seed=1))
+            s.step(args.reps)
+        s.sync()
+    print(f"kernel-only {args.kernel_only} {n}^3 {args.precision} x{args.reps}: done")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "step"], default=None,
+                    help="launch one kernel family a few times (for profilers) and exit")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--shape", type=int, default=N)
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
+    if args.kernel_only:
+        return run_kernel_only(args)
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))
