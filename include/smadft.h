@@ -165,12 +165,12 @@ int smadft_get_stream(smadft_ctx *ctx, void **stream);
 int smadft_launch_count(const smadft_ctx *ctx, long long *count);
 
 /* One axis pass of a 3-D r2r transform on device buffers (axis 0=x, 1=y, 2=z; kind as
- * below); in may equal out.  Exposed for tuning and for per-kernel roofline timing. */
+ * below); in may equal out; both 16-byte aligned.  Exposed for tuning and for per-kernel roofline timing. */
 int smadft_r2r_pass_device(smadft_ctx *ctx, const void *in, void *out, int axis, int kind);
 
 /* Stand-alone 3-D r2r transform on device buffers (what fftw_execute does for one plan,
  * e.g. no-adv/cosNoAdvTrackSing.cpp:727).  kinds: 0 REDFT10, 1 REDFT01, 2 RODFT10,
- * 3 RODFT01 per axis; in may equal out.  precision SMADFT_FP64 (double*) or SMADFT_FP32
+ * 3 RODFT01 per axis; in may equal out; both 16-byte aligned.  precision SMADFT_FP64 (double*) or SMADFT_FP32
  * (float*).  Uses the context's stream and scratch field; the context's grid must match. */
 int smadft_r2r3d_device(smadft_ctx *ctx, const void *in, void *out, int kx, int ky, int kz);
 

@@ -21,14 +21,22 @@ __device__ __forceinline__ T nl3(T p, T beta, T gamma)   // beta psi^3 - gamma p
 }
 
 // ---------------------------------------------------------------- loaders -------------
+// All functors follow the vector interface of r2r_pass.cuh: V consecutive elements along z
+// (idx .. idx+V-1 at (i, j, k .. k+V-1)); same-index fields use 16-byte loads, index-shifted
+// neighbours along z use scalar loads.
+
 // N = beta psi^3 - gamma psi^5 (no-adv/cosNoAdvTrackSing.cpp:713-723)
 template <typename T>
 struct LdNonlin {
     const T *__restrict__ psi;
     T beta, gamma;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
     {
-        return nl3(psi[q], beta, gamma);
+        T p[V];
+        vld<T, V>(psi, q, p);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = nl3(p[u], beta, gamma);
     }
 };
 
@@ -38,11 +46,25 @@ template <typename T, int AX>
 struct LdGrad {
     Spec<T> s;
     const T *__restrict__ f;
-    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
-        if (AX == 0) return (i < s.nx - 1) ? -s.sx[i] * f[q + s.nyz] : T(0);
-        if (AX == 1) return (j < s.ny - 1) ? -s.sy[j] * f[q + s.nz] : T(0);
-        return (k < s.nz - 1) ? -s.sz[k] * f[q + 1] : T(0);
+        if (AX == 0 || AX == 1) {
+            const bool in = AX == 0 ? (i < s.nx - 1) : (j < s.ny - 1);
+            if (!in) {
+#pragma unroll
+                for (int u = 0; u < V; u++) out[u] = T(0);
+                return;
+            }
+            T v[V];
+            vld<T, V>(f, q + (AX == 0 ? s.nyz : (long long)s.nz), v);
+            const T sc = AX == 0 ? s.sx[i] : s.sy[j];
+#pragma unroll
+            for (int u = 0; u < V; u++) out[u] = -sc * v[u];
+        } else {
+#pragma unroll
+            for (int u = 0; u < V; u++) out[u] = (k + u < s.nz - 1) ? -s.sz[k + u] * f[q + u + 1] : T(0);
+        }
     }
 };
 
@@ -51,9 +73,13 @@ template <typename T>
 struct LdNegLin {
     Spec<T> s;
     const T *__restrict__ ph;
-    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
-        return -s.alin(i, j, k) * ph[q];
+        T v[V];
+        vld<T, V>(ph, q, v);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = -s.alin(i, j, k + u) * v[u];
     }
 };
 
@@ -62,9 +88,15 @@ template <typename T>
 struct LdForce {
     const T *__restrict__ psi, *__restrict__ sp2, *__restrict__ g;
     T beta, gamma;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
     {
-        return (sp2[q] - nl3(psi[q], beta, gamma)) * g[q];
+        T a[V], b[V], c[V];
+        vld<T, V>(psi, q, a);
+        vld<T, V>(sp2, q, b);
+        vld<T, V>(g, q, c);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = (b[u] - nl3(a[u], beta, gamma)) * c[u];
     }
 };
 
@@ -73,47 +105,95 @@ struct LdForce {
 //   v_x[i,j,k] = CM1x (Sx - CM2x (s_i Sx + q_j Sy[i+1,j-1,k] + q_k Sz[i+1,j,k-1])), i < nx-1
 //   v_y[i,j,k] = CM1y (Sy - CM2y (q_i Sx[i-1,j+1,k] + s_j Sy + q_k Sz[i,j+1,k-1])), j<ny-1, k<nz-1
 //   v_z[i,j,k] = CM1z (Sz - CM2z (q_i Sx[i-1,j,k+1] + q_j Sy[i,j-1,k+1] + s_k Sz)), j<ny-1, k<nz-1
-// with CM1 = scale / (nu |q_s|^2), CM2 = s / |q_s|^2 and index -1 neighbours = 0.
+// with CM1 = scale / (nu |q_s|^2), CM2 = s / |q_s|^2 (one reciprocal) and index -1
+// neighbours = 0.
 template <typename T, int AX, bool DIVV>
 struct LdStokes {
     Spec<T> s;
     const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz, *__restrict__ dv;
-    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
+        const T snu = s.scale / s.nu;
         if (AX == 0) {
-            if (i >= s.nx - 1) return T(0);
+            if (i >= s.nx - 1) {
+#pragma unroll
+                for (int u = 0; u < V; u++) out[u] = T(0);
+                return;
+            }
             const long long qn = q + s.nyz;   // (i+1, j, k)
-            T sy = (j != 0) ? Sy[qn - s.nz] : T(0);
-            T sz = (k != 0) ? Sz[qn - 1] : T(0);
-            T m2 = s.sx[i] * s.sx[i] + s.qy[j] * s.qy[j] + s.qz[k] * s.qz[k];
-            T cm1 = s.scale / (s.nu * m2), cm2 = s.sx[i] / m2;
-            T sxv = Sx[q];
-            T dot = s.sx[i] * sxv + s.qy[j] * sy + s.qz[k] * sz;
-            T v = cm1 * (sxv - cm2 * dot);
-            if (DIVV) v = v + cm1 * (s.nu * s.sx[i] * dv[qn]);
-            return v;
+            T sx[V], sy[V], d[V];
+            vld<T, V>(Sx, q, sx);
+            if (j != 0) vld<T, V>(Sy, qn - s.nz, sy);
+            else {
+#pragma unroll
+                for (int u = 0; u < V; u++) sy[u] = T(0);
+            }
+            if (DIVV) vld<T, V>(dv, qn, d);
+            const T si = s.sx[i], qj = s.qy[j];
+            const T a2 = si * si + qj * qj;
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const int kk = k + u;
+                const T qk = s.qz[kk];
+                const T sz = (kk != 0) ? Sz[qn - 1 + u] : T(0);
+                const T inv = T(1) / (a2 + qk * qk);
+                const T dot = si * sx[u] + qj * sy[u] + qk * sz;
+                T v = snu * inv * (sx[u] - si * inv * dot);
+                if (DIVV) v = v + snu * inv * (s.nu * si * d[u]);
+                out[u] = v;
+            }
         } else if (AX == 1) {
-            if (j >= s.ny - 1 || k >= s.nz - 1) return T(0);
-            T sx = (i != 0) ? Sx[q - s.nyz + s.nz] : T(0);          // (i-1, j+1, k)
-            T sz = (k != 0) ? Sz[q + s.nz - 1] : T(0);              // (i, j+1, k-1)
-            T m2 = s.qx[i] * s.qx[i] + s.sy[j] * s.sy[j] + s.qz[k] * s.qz[k];
-            T cm1 = s.scale / (s.nu * m2), cm2 = s.sy[j] / m2;
-            T syv = Sy[q];
-            T dot = s.qx[i] * sx + s.sy[j] * syv + s.qz[k] * sz;
-            T v = cm1 * (syv - cm2 * dot);
-            if (DIVV) v = v + cm1 * (s.nu * s.sy[j] * dv[q + s.nz]);
-            return v;
+            if (j >= s.ny - 1) {
+#pragma unroll
+                for (int u = 0; u < V; u++) out[u] = T(0);
+                return;
+            }
+            T syv[V], sx[V], d[V];
+            vld<T, V>(Sy, q, syv);
+            if (i != 0) vld<T, V>(Sx, q - s.nyz + s.nz, sx);              // (i-1, j+1, k)
+            else {
+#pragma unroll
+                for (int u = 0; u < V; u++) sx[u] = T(0);
+            }
+            if (DIVV) vld<T, V>(dv, q + s.nz, d);
+            const T qi = s.qx[i], sj = s.sy[j];
+            const T a2 = qi * qi + sj * sj;
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const int kk = k + u;
+                if (kk >= s.nz - 1) { out[u] = T(0); continue; }
+                const T qk = s.qz[kk];
+                const T sz = (kk != 0) ? Sz[q + s.nz - 1 + u] : T(0);      // (i, j+1, k-1)
+                const T inv = T(1) / (a2 + qk * qk);
+                const T dot = qi * sx[u] + sj * syv[u] + qk * sz;
+                T v = snu * inv * (syv[u] - sj * inv * dot);
+                if (DIVV) v = v + snu * inv * (s.nu * sj * d[u]);
+                out[u] = v;
+            }
         } else {
-            if (j >= s.ny - 1 || k >= s.nz - 1) return T(0);
-            T sx = (i != 0) ? Sx[q - s.nyz + 1] : T(0);             // (i-1, j, k+1)
-            T sy = (j != 0) ? Sy[q - s.nz + 1] : T(0);              // (i, j-1, k+1)
-            T m2 = s.qx[i] * s.qx[i] + s.qy[j] * s.qy[j] + s.sz[k] * s.sz[k];
-            T cm1 = s.scale / (s.nu * m2), cm2 = s.sz[k] / m2;
-            T szv = Sz[q];
-            T dot = s.qx[i] * sx + s.qy[j] * sy + s.sz[k] * szv;
-            T v = cm1 * (szv - cm2 * dot);
-            if (DIVV) v = v + cm1 * (s.nu * s.sz[k] * dv[q + 1]);
-            return v;
+            if (j >= s.ny - 1) {
+#pragma unroll
+                for (int u = 0; u < V; u++) out[u] = T(0);
+                return;
+            }
+            T szv[V];
+            vld<T, V>(Sz, q, szv);
+            const T qi = s.qx[i], qj = s.qy[j];
+            const T a2 = qi * qi + qj * qj;
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const int kk = k + u;
+                if (kk >= s.nz - 1) { out[u] = T(0); continue; }
+                const T sk = s.sz[kk];
+                const T sx = (i != 0) ? Sx[q - s.nyz + 1 + u] : T(0);      // (i-1, j, k+1)
+                const T sy = (j != 0) ? Sy[q - s.nz + 1 + u] : T(0);       // (i, j-1, k+1)
+                const T inv = T(1) / (a2 + sk * sk);
+                const T dot = qi * sx + qj * sy + sk * szv[u];
+                T v = snu * inv * (szv[u] - sk * inv * dot);
+                if (DIVV) v = v + snu * inv * (s.nu * sk * dv[q + 1 + u]);
+                out[u] = v;
+            }
         }
     }
 };
@@ -124,9 +204,16 @@ struct LdAdvN {
     const T *__restrict__ psi, *__restrict__ vx, *__restrict__ vy, *__restrict__ vz;
     const T *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
     T beta, gamma;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
     {
-        return nl3(psi[q], beta, gamma) - vx[q] * gx[q] - vy[q] * gy[q] - vz[q] * gz[q];
+        T p[V], a[V], b[V], c[V], d[V], e[V], f[V];
+        vld<T, V>(psi, q, p);
+        vld<T, V>(vx, q, a); vld<T, V>(gx, q, d);
+        vld<T, V>(vy, q, b); vld<T, V>(gy, q, e);
+        vld<T, V>(vz, q, c); vld<T, V>(gz, q, f);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = nl3(p[u], beta, gamma) - a[u] * d[u] - b[u] * e[u] - c[u] * f[u];
     }
 };
 
@@ -139,13 +226,20 @@ struct StUpdCN {
     Spec<T> s;
     T *__restrict__ ph;
     T *__restrict__ np;
-    __device__ __forceinline__ void operator()(long long q, int i, int j, int k, T v) const
+    template <int V>
+    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
-        T al = s.alin(i, j, k);
-        T c1 = T(1) + s.dtd2 * al, c2 = T(1) - s.dtd2 * al;
-        T npv = np[q];
-        ph[q] = (c1 * ph[q] + s.dtd2 * s.scale * (T(3) * v - npv)) / c2;
-        np[q] = v;
+        T p[V], n0[V], o[V];
+        vld<T, V>(ph, q, p);
+        vld<T, V>(np, q, n0);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            const T al = s.alin(i, j, k + u);
+            const T c1 = T(1) + s.dtd2 * al, c2 = T(1) - s.dtd2 * al;
+            o[u] = (c1 * p[u] + s.dtd2 * s.scale * (T(3) * v[u] - n0[u])) / c2;
+        }
+        vst<T, V>(ph, q, o);
+        vst<T, V>(np, q, v);
     }
 };
 
@@ -154,7 +248,14 @@ template <typename T>
 struct StScale {
     T *__restrict__ p;
     T scale;
-    __device__ __forceinline__ void operator()(long long q, int, int, int, T v) const { p[q] = scale * v; }
+    template <int V>
+    __device__ __forceinline__ void store(long long q, int, int, int, const T *v) const
+    {
+        T o[V];
+#pragma unroll
+        for (int u = 0; u < V; u++) o[u] = scale * v[u];
+        vst<T, V>(p, q, o);
+    }
 };
 
 }  // namespace smadft

@@ -14,9 +14,13 @@ template <typename T>
 struct LdDfd {
     Spec<T> s;
     const T *__restrict__ ph;
-    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
-        return s.alpha * (s.q02 - s.mq2(i, j, k)) * ph[q];
+        T v[V];
+        vld<T, V>(ph, q, v);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = s.alpha * (s.q02 - s.mq2(i, j, k + u)) * v[u];
     }
 };
 
@@ -25,10 +29,16 @@ template <typename T>
 struct LdLapDfd {
     Spec<T> s;
     const T *__restrict__ ph;
-    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
-        T m = s.mq2(i, j, k);
-        return -m * s.alpha * (s.q02 - m) * ph[q];
+        T v[V];
+        vld<T, V>(ph, q, v);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            const T m = s.mq2(i, j, k + u);
+            out[u] = -m * s.alpha * (s.q02 - m) * v[u];
+        }
     }
 };
 
@@ -37,10 +47,14 @@ template <typename T>
 struct LdRhoRaw {
     const T *__restrict__ psi, *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
     T kp, rho0, q02;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
     {
-        T p = psi[q], a = gx[q], b = gy[q], c = gz[q];
-        return kp * sqrt(q02 * (p * p) + a * a + b * b + c * c) + rho0;
+        T p[V], a[V], b[V], c[V];
+        vld<T, V>(psi, q, p); vld<T, V>(gx, q, a); vld<T, V>(gy, q, b); vld<T, V>(gz, q, c);
+#pragma unroll
+        for (int u = 0; u < V; u++)
+            out[u] = kp * sqrt(q02 * (p[u] * p[u]) + a[u] * a[u] + b[u] * b[u] + c[u] * c[u]) + rho0;
     }
 };
 
@@ -49,9 +63,14 @@ template <typename T>
 struct StFilter {
     Spec<T> s;
     T *__restrict__ out;
-    __device__ __forceinline__ void operator()(long long q, int i, int j, int k, T v) const
+    template <int V>
+    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
-        out[q] = (s.scale * v) * (s.ex[i] * s.ey[j] * s.ez[k]);
+        T o[V];
+        const T exy = s.ex[i] * s.ey[j];
+#pragma unroll
+        for (int u = 0; u < V; u++) o[u] = (s.scale * v[u]) * (exy * s.ez[k + u]);
+        vst<T, V>(out, q, o);
     }
 };
 
@@ -61,17 +80,32 @@ struct LdDivv {
     const T *__restrict__ rho, *__restrict__ ro, *__restrict__ vx, *__restrict__ vy, *__restrict__ vz;
     const T *__restrict__ rx, *__restrict__ ry, *__restrict__ rz;
     T dt;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
     {
-        T r = rho[q], o = ro[q];
-        return -((r - o) / dt + vx[q] * rx[q] + vy[q] * ry[q] + vz[q] * rz[q]) / (T(0.5) * (r + o));
+        T r[V], o[V], a[V], b[V], c[V], d[V], e[V], f[V];
+        vld<T, V>(rho, q, r); vld<T, V>(ro, q, o);
+        vld<T, V>(vx, q, a); vld<T, V>(rx, q, d);
+        vld<T, V>(vy, q, b); vld<T, V>(ry, q, e);
+        vld<T, V>(vz, q, c); vld<T, V>(rz, q, f);
+#pragma unroll
+        for (int u = 0; u < V; u++)
+            out[u] = -((r[u] - o[u]) / dt + a[u] * d[u] + b[u] * e[u] + c[u] * f[u]) / (T(0.5) * (r[u] + o[u]));
     }
 };
 
 template <typename T>
 struct LdMul {
     const T *__restrict__ a, *__restrict__ b;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const { return a[q] * b[q]; }
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    {
+        T x[V], y[V];
+        vld<T, V>(a, q, x);
+        vld<T, V>(b, q, y);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = x[u] * y[u];
+    }
 };
 
 // lap <- -scale q^2 REDFT10^3(rho f') (quasi/quasi.cpp:1392-1400)
@@ -79,9 +113,13 @@ template <typename T>
 struct StLapSpec {
     Spec<T> s;
     T *__restrict__ out;
-    __device__ __forceinline__ void operator()(long long q, int i, int j, int k, T v) const
+    template <int V>
+    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
-        out[q] = -s.scale * s.mq2(i, j, k) * v;
+        T o[V];
+#pragma unroll
+        for (int u = 0; u < V; u++) o[u] = -s.scale * s.mq2(i, j, k + u) * v[u];
+        vst<T, V>(out, q, o);
     }
 };
 
@@ -94,18 +132,26 @@ struct LdQForce {
     T *__restrict__ mu_out, *__restrict__ en_out;
     T eps, beta, gamma;
     int lap_rho;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
     {
-        T ps = psi[q], f = dfd[q], rh = rho[q];
-        T p2 = ps * ps, p3 = p2 * ps, p4 = p2 * p2;
-        T e = T(-0.5) * eps * p2 + T(0.5) * (f * f) - T(0.25) * beta * p4 + (gamma / T(6)) * (p4 * p2);
-        T lv = lap_rho ? rh * lap[q] : lap[q];
-        T m = lv + rh * (f - eps * ps - beta * p3 + gamma * (p3 * p2));
-        if (AX == 0) {
-            mu_out[q] = m;
-            en_out[q] = e;
+        T ps[V], f[V], lp[V], rh[V], gg[V], rr[V], mo[V], eo[V];
+        vld<T, V>(psi, q, ps); vld<T, V>(dfd, q, f); vld<T, V>(lap, q, lp); vld<T, V>(rho, q, rh);
+        vld<T, V>(g, q, gg); vld<T, V>(r, q, rr);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            const T p = ps[u], p2 = p * p, p3 = p2 * p, p4 = p2 * p2;
+            const T e = T(-0.5) * eps * p2 + T(0.5) * (f[u] * f[u]) - T(0.25) * beta * p4 + (gamma / T(6)) * (p4 * p2);
+            const T lv = lap_rho ? rh[u] * lp[u] : lp[u];
+            const T m = lv + rh[u] * (f[u] - eps * p - beta * p3 + gamma * (p3 * p2));
+            mo[u] = m;
+            eo[u] = e;
+            out[u] = m * gg[u] + e * rr[u];
         }
-        return m * g[q] + e * r[q];
+        if (AX == 0) {
+            vst<T, V>(mu_out, q, mo);
+            vst<T, V>(en_out, q, eo);
+        }
     }
 };
 
@@ -114,14 +160,20 @@ template <typename T>
 struct LdPressure {
     Spec<T> s;
     const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz, *__restrict__ dv;
-    __device__ __forceinline__ T operator()(long long q, int i, int j, int k) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
-        if (i + j + k == 0) return T(0);
-        T sx = (i > 0) ? Sx[q - s.nyz] : T(0);
-        T sy = (j > 0) ? Sy[q - s.nz] : T(0);
-        T sz = (k > 0) ? Sz[q - 1] : T(0);
-        return s.scale * (-(s.qx[i] * sx + s.qy[j] * sy + s.qz[k] * sz) / s.mq2(i, j, k) +
-                          (s.lam + T(2) * s.nu) * dv[q]);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            const int kk = k + u;
+            const long long qq = q + u;
+            if (i + j + kk == 0) { out[u] = T(0); continue; }
+            const T sx = (i > 0) ? Sx[qq - s.nyz] : T(0);
+            const T sy = (j > 0) ? Sy[qq - s.nz] : T(0);
+            const T sz = (kk > 0) ? Sz[qq - 1] : T(0);
+            out[u] = s.scale * (-(s.qx[i] * sx + s.qy[j] * sy + s.qz[kk] * sz) / s.mq2(i, j, kk) +
+                                (s.lam + T(2) * s.nu) * dv[qq]);
+        }
     }
 };
 
@@ -135,14 +187,23 @@ struct LdQN {
     const T *__restrict__ rx, *__restrict__ ry, *__restrict__ rz;
     T kp;
     int extra;
-    __device__ __forceinline__ T operator()(long long q, int, int, int) const
+    template <int V>
+    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
     {
-        T v = -mu[q] - vx[q] * gx[q] - vy[q] * gy[q] - vz[q] * gz[q];
+        T m[V], a[V], b[V], c[V], d[V], e[V], f[V];
+        vld<T, V>(mu, q, m);
+        vld<T, V>(vx, q, a); vld<T, V>(gx, q, d);
+        vld<T, V>(vy, q, b); vld<T, V>(gy, q, e);
+        vld<T, V>(vz, q, c); vld<T, V>(gz, q, f);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = -m[u] - a[u] * d[u] - b[u] * e[u] - c[u] * f[u];
         if (extra) {
-            T a = rx[q], b = ry[q], c = rz[q], r = rho[q];
-            v += (p[q] + r * en[q]) * kp * sqrt(a * a + b * b + c * c) / (r * r);
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const T x = rx[q + u], y = ry[q + u], z = rz[q + u], r = rho[q + u];
+                out[u] += (p[q + u] + r * en[q + u]) * kp * sqrt(x * x + y * y + z * z) / (r * r);
+            }
         }
-        return v;
     }
 };
 
@@ -153,15 +214,23 @@ struct StUpdBDF {
     Spec<T> s;
     T *__restrict__ ph, *__restrict__ pho, *__restrict__ np;
     int first;
-    __device__ __forceinline__ void operator()(long long q, int i, int j, int k, T v) const
+    template <int V>
+    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
-        T al = s.alin(i, j, k);
-        T c1 = T(2) - s.dt * s.rho_m * al, c2 = T(1.5) - s.dt * s.rho_m * al;
-        T npv = first ? v : np[q];
-        T old = ph[q];
-        ph[q] = (c1 * old - T(0.5) * pho[q] + s.dtd2 * s.scale * (T(3) * v - npv)) / c2;
-        pho[q] = old;
-        np[q] = v;
+        T old[V], oo[V], n0[V], o[V];
+        vld<T, V>(ph, q, old);
+        vld<T, V>(pho, q, oo);
+        vld<T, V>(np, q, n0);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            const T al = s.alin(i, j, k + u);
+            const T c1 = T(2) - s.dt * s.rho_m * al, c2 = T(1.5) - s.dt * s.rho_m * al;
+            const T npv = first ? v[u] : n0[u];
+            o[u] = (c1 * old[u] - T(0.5) * oo[u] + s.dtd2 * s.scale * (T(3) * v[u] - npv)) / c2;
+        }
+        vst<T, V>(ph, q, o);
+        vst<T, V>(pho, q, old);
+        vst<T, V>(np, q, v);
     }
 };
 

@@ -155,6 +155,8 @@ __device__ __forceinline__ void codelet(cpx<T> *v)
 }
 
 // One in-place DIF stage of radix R over `nl` lines: block size M (= R * stride).
+// In every plan each stage's stride is a multiple of the last radix RL (or the stage is the
+// last one and its block base is), so phys(base + q STR) = phys(base) + q (STR + STR/RL).
 template <typename T, int N, int R, int M, bool INV>
 __device__ __forceinline__ void dif_stage(cpx<T> *__restrict__ buf, int nl, const cpx<T> *__restrict__ w)
 {
@@ -162,23 +164,25 @@ __device__ __forceinline__ void dif_stage(cpx<T> *__restrict__ buf, int nl, cons
     constexpr int STR = M / R;              // butterfly stride
     constexpr int PER_LINE = N / R;         // butterflies per line
     constexpr int TW = N / M;               // twiddle table step: W_M^e = W_N^(e TW)
+    constexpr int DP = STR + STR / PI::RL;  // physical distance between the R points
     const int tasks = nl * PER_LINE;
     for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
         const int c = t / PER_LINE;
         const int u = t - c * PER_LINE;
         const int b = u / STR;
         const int j = u - b * STR;
-        cpx<T> *line = buf + c * PI::LD;
-        const int base = b * M + j;
+        cpx<T> *pt = buf + c * PI::LD + PI::phys(b * M + j);
         cpx<T> v[R];
 #pragma unroll
-        for (int q = 0; q < R; q++) v[q] = line[PI::phys(base + q * STR)];
+        for (int q = 0; q < R; q++) v[q] = pt[q * DP];
         codelet<R, T, INV>(v);
+        pt[0] = v[0];
+        const int jt = j * TW;
 #pragma unroll
-        for (int q = 0; q < R; q++) {
+        for (int q = 1; q < R; q++) {
             cpx<T> o = v[q];
-            if (STR > 1 && q > 0 && j > 0) o = cmul(o, tw<T, INV>(w, j * q * TW));
-            line[PI::phys(base + q * STR)] = o;
+            if (STR > 1) o = cmul(o, tw<T, INV>(w, jt * q));
+            pt[q * DP] = o;
         }
     }
 }
@@ -258,6 +262,14 @@ constexpr int batch_size(int per)
 template <typename T, int N>
 constexpr size_t fast_smem_bytes() { return ((size_t)(kFastW / 2) * PlanInfo<N>::LD + 2 * N) * sizeof(cpx<T>); }
 
+// Post-twiddle of a forward (DCT-II) transform: output for line part `odd` (0 = real line A,
+// 1 = real line B) from Z[k] and Z[N-k] of the packed complex line (see fft_tile.cuh).
+template <typename T>
+__device__ __forceinline__ T dct2_out(cpx<T> zk, cpx<T> zm, cpx<T> hh, int odd)
+{
+    return odd ? hh.x * (zk.y + zm.y) - hh.y * (zk.x - zm.x) : hh.x * (zk.x + zm.x) + hh.y * (zk.y - zm.y);
+}
+
 template <typename T, int N, int AXIS, class LD, class ST>
 __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int kind, int tiles_b,
                                                                    const cpx<T> *__restrict__ wt_g,
@@ -265,9 +277,10 @@ __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int k
 {
     using PI = PlanInfo<N>;
     constexpr int W = kFastW, NL = W / 2;
-    constexpr int PER = N * W / kFastThreads;     // tile elements per thread
-    constexpr int BATCH = batch_size(PER);        // loads in flight per thread
-    static_assert(PER % BATCH == 0, "tile must split evenly");
+    constexpr int V = 16 / sizeof(T);             // elements per 16-byte global access
+    constexpr int PERV = N * W / V / kFastThreads; // vector accesses per thread
+    constexpr int BATCH = batch_size(PERV);
+    static_assert(PERV % BATCH == 0, "tile must split evenly");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T> *buf = reinterpret_cast<cpx<T> *>(smem_raw);
     cpx<T> *wt = buf + NL * PI::LD;               // FFT twiddles W_N^m
@@ -275,34 +288,61 @@ __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int k
     T *rb = reinterpret_cast<T *>(smem_raw);
     const TileBase tb = tile_base<AXIS>(g, W, tiles_b);
     const bool fwd = (kind == K_DCT2 || kind == K_DST2);
+    const bool sine = (kind == K_DST2 || kind == K_DST3);
+    // 16-byte accesses need V | nz (element index alignment); otherwise V = 1 accesses
+    const bool vec_ok = (g.nz % V) == 0;
     for (int m = threadIdx.x; m < N; m += kFastThreads) {
         wt[m] = wt_g[m];
         ht[m] = ht_g[m];
     }
 
-    // ---- global -> shared, input permutation per kind; BATCH independent loads per thread
+    // ---- global -> shared.  A vector access covers V consecutive k: V consecutive line
+    // positions t (z axis) or V consecutive lines w (x, y axes).  Partial tiles (nz not a
+    // multiple of W) fall back to V = 1 accesses through the same code.
 #pragma unroll 1
-    for (int e0 = 0; e0 < PER; e0 += BATCH) {
-        T vals[BATCH];
-        int spos[BATCH];
+    for (int e0 = 0; e0 < PERV; e0 += BATCH) {
+        T vals[BATCH][V];
+        int tt[BATCH], ww[BATCH];
 #pragma unroll
         for (int b = 0; b < BATCH; b++) {
             const int e = (e0 + b) * kFastThreads + threadIdx.x;
             int t, w;
-            if (AXIS == 2) { t = e % N; w = e / N; }
-            else { w = e % W; t = e / W; }
+            if (AXIS == 2) { t = (e % (N / V)) * V; w = e / (N / V); }
+            else { w = (e % (W / V)) * V; t = e / (W / V); }
+            tt[b] = t;
+            ww[b] = w;
             const ElemPos p = tile_elem<AXIS>(g, tb, t, w);
-            T v = p.valid ? ld(p.idx, p.i, p.j, p.k) : T(0);
-            int pos;
-            if (kind == K_DCT2) pos = makhoul_pos(t, N);
-            else if (kind == K_DST2) { pos = makhoul_pos(t, N); if (t & 1) v = -v; }
-            else if (kind == K_DCT3) pos = t;
-            else pos = N - 1 - t;
-            vals[b] = v;
-            spos[b] = 2 * ((w >> 1) * PI::LD + PI::phys(pos)) + (w & 1);
+            if (vec_ok && (AXIS == 2 || p.k + V <= g.nz)) {
+                if (p.valid) ld.template load<V>(p.idx, p.i, p.j, p.k, vals[b]);
+                else {
+#pragma unroll
+                    for (int u = 0; u < V; u++) vals[b][u] = T(0);
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < V; u++) {
+                    if (p.k + u < g.nz) ld.template load<1>(p.idx + u, p.i, p.j, p.k + u, &vals[b][u]);
+                    else vals[b][u] = T(0);
+                }
+            }
         }
 #pragma unroll
-        for (int b = 0; b < BATCH; b++) rb[spos[b]] = vals[b];
+        for (int b = 0; b < BATCH; b++) {
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const int t = AXIS == 2 ? tt[b] + u : tt[b];
+                const int w = AXIS == 2 ? ww[b] : ww[b] + u;
+                T v = vals[b][u];
+                int pos;
+                if (fwd) {
+                    pos = makhoul_pos(t, N);
+                    if (sine && (t & 1)) v = -v;
+                } else {
+                    pos = sine ? N - 1 - t : t;
+                }
+                rb[2 * ((w >> 1) * PI::LD + PI::phys(pos)) + (w & 1)] = v;
+            }
+        }
     }
     __syncthreads();
 
@@ -340,27 +380,36 @@ __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int k
     }
 
     // ---- shared -> global, output permutation / post-twiddle per kind
-    for (int e = threadIdx.x; e < N * W; e += kFastThreads) {
+    for (int e = threadIdx.x; e < N * W / V; e += kFastThreads) {
         int o, w;
-        if (AXIS == 2) { o = e % N; w = e / N; }
-        else { w = e % W; o = e / W; }
+        if (AXIS == 2) { o = (e % (N / V)) * V; w = e / (N / V); }
+        else { w = (e % (W / V)) * V; o = e / (W / V); }
         const ElemPos p = tile_elem<AXIS>(g, tb, o, w);
-        const cpx<T> *L = buf + (w >> 1) * PI::LD;
-        T v;
-        if (fwd) {
-            const int k = (kind == K_DCT2) ? o : (N - 1 - o);
-            const cpx<T> zk = L[PI::phys(PI::pos(k))];
-            const cpx<T> zm = L[PI::phys(PI::pos(k == 0 ? 0 : N - k))];
-            const cpx<T> hh = ht[k];
-            const T cc = hh.x, ss = hh.y;
-            if ((w & 1) == 0) v = cc * (zk.x + zm.x) + ss * (zk.y - zm.y);
-            else v = cc * (zk.y + zm.y) - ss * (zk.x - zm.x);
-        } else {
-            const cpx<T> z = L[PI::phys(PI::pos(makhoul_pos(o, N)))];
-            v = (w & 1) ? z.y : z.x;
-            if (kind == K_DST3 && (o & 1)) v = -v;
+        T v[V];
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            const int oo = AXIS == 2 ? o + u : o;
+            const int wu = AXIS == 2 ? w : w + u;
+            const cpx<T> *L = buf + (wu >> 1) * PI::LD;
+            if (fwd) {
+                const int k = sine ? (N - 1 - oo) : oo;
+                const cpx<T> zk = L[PI::phys(PI::pos(k))];
+                const cpx<T> zm = L[PI::phys(PI::pos(k == 0 ? 0 : N - k))];
+                v[u] = dct2_out(zk, zm, ht[k], wu & 1);
+            } else {
+                const cpx<T> z = L[PI::phys(PI::pos(makhoul_pos(oo, N)))];
+                T r = (wu & 1) ? z.y : z.x;
+                v[u] = (sine && (oo & 1)) ? -r : r;
+            }
         }
-        if (p.valid) st(p.idx, p.i, p.j, p.k, v);
+        if (!p.valid) continue;
+        if (vec_ok && (AXIS == 2 || p.k + V <= g.nz)) {
+            st.template store<V>(p.idx, p.i, p.j, p.k, v);
+        } else {
+#pragma unroll
+            for (int u = 0; u < V; u++)
+                if (p.k + u < g.nz) st.template store<1>(p.idx + u, p.i, p.j, p.k + u, &v[u]);
+        }
     }
 }
 

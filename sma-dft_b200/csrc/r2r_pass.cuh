@@ -65,16 +65,50 @@ __device__ __forceinline__ ElemPos elem_pos(const PassArgs<T> &a, int t, int w)
     return e;
 }
 
-// Identity loader / storer on a plain array.
+// V consecutive elements p[idx .. idx+V-1]; for V > 1, idx is a multiple of V and p is
+// 16-byte aligned (one 16-byte access: float4 / double2).
+template <typename T, int V>
+__device__ __forceinline__ void vld(const T *__restrict__ p, long long idx, T *o)
+{
+    if constexpr (V == 4 && sizeof(T) == 4) {
+        const float4 u = *reinterpret_cast<const float4 *>(p + idx);
+        o[0] = u.x; o[1] = u.y; o[2] = u.z; o[3] = u.w;
+    } else if constexpr (V == 2 && sizeof(T) == 8) {
+        const double2 u = *reinterpret_cast<const double2 *>(p + idx);
+        o[0] = u.x; o[1] = u.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < V; q++) o[q] = p[idx + q];
+    }
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void vst(T *__restrict__ p, long long idx, const T *v)
+{
+    if constexpr (V == 4 && sizeof(T) == 4) {
+        *reinterpret_cast<float4 *>(p + idx) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (V == 2 && sizeof(T) == 8) {
+        *reinterpret_cast<double2 *>(p + idx) = make_double2(v[0], v[1]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < V; q++) p[idx + q] = v[q];
+    }
+}
+
+// Functor interface of the pass kernels.  A loader fills out[0..V-1] with the transform
+// input at (i, j, k+u), u < V (memory idx+u, consecutive along z); a storer consumes the
+// transform output for the same V elements.
 template <typename T>
 struct LoadArr {
     const T *__restrict__ p;
-    __device__ __forceinline__ T operator()(long long idx, int, int, int) const { return p[idx]; }
+    template <int V>
+    __device__ __forceinline__ void load(long long idx, int, int, int, T *out) const { vld<T, V>(p, idx, out); }
 };
 template <typename T>
 struct StoreArr {
     T *__restrict__ p;
-    __device__ __forceinline__ void operator()(long long idx, int, int, int, T v) const { p[idx] = v; }
+    template <int V>
+    __device__ __forceinline__ void store(long long idx, int, int, int, const T *v) const { vst<T, V>(p, idx, v); }
 };
 
 template <typename T, class LD, class ST>
@@ -97,7 +131,8 @@ __global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST 
         if (a.axis == 2) { t = e % n; w = e / n; }
         else { w = e % W; t = e / W; }
         ElemPos p = elem_pos(a, t, w);
-        T v = p.valid ? ld(p.idx, p.i, p.j, p.k) : T(0);
+        T v = T(0);
+        if (p.valid) ld.template load<1>(p.idx, p.i, p.j, p.k, &v);
         int pos;
         if (kind == K_DCT2) pos = makhoul_pos(t, n);
         else if (kind == K_DST2) { pos = makhoul_pos(t, n); if (t & 1) v = -v; }
@@ -151,7 +186,7 @@ __global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST 
             v = (w & 1) ? z.y : z.x;
             if (kind == K_DST3 && (o & 1)) v = -v;
         }
-        if (p.valid) st(p.idx, p.i, p.j, p.k, v);
+        if (p.valid) st.template store<1>(p.idx, p.i, p.j, p.k, &v);
     }
 }
 

@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <string>
@@ -625,6 +626,7 @@ int smadft_launch_count(const smadft_ctx *h, long long *count)
 int smadft_r2r_pass_device(smadft_ctx *h, const void *in, void *out, int axis, int kind)
 {
     if (!h || !in || !out || axis < 0 || axis > 2 || kind < 0 || kind > 3) return SMADFT_ERR_INVALID;
+    if (((uintptr_t)in | (uintptr_t)out) & 15) return fail(h->c, SMADFT_ERR_INVALID, "buffers must be 16-byte aligned");
     Ctx &c = h->c;
     cudaSetDevice(c.dev);
     if (c.f32)
@@ -638,6 +640,7 @@ int smadft_r2r3d_device(smadft_ctx *h, const void *in, void *out, int kx, int ky
     for (int k : {kx, ky, kz})
         if (k < 0 || k > 3) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
+    if (((uintptr_t)in | (uintptr_t)out) & 15) return fail(c, SMADFT_ERR_INVALID, "buffers must be 16-byte aligned");
     cudaSetDevice(c.dev);
     if (c.f32)
         return r2r3d<float>(c, kx, ky, kz, LoadArr<float>{(const float *)in}, StoreArr<float>{(float *)out});
