@@ -42,6 +42,7 @@ extern "C" {
 #define SMADFT_ERR_IO -7           /* checkpoint file could not be read or written          */
 #define SMADFT_ERR_STATE -8        /* call out of order (e.g. step before set_psi)          */
 #define SMADFT_ERR_NODEVICE -9     /* no CUDA device / extension not usable                 */
+#define SMADFT_ERR_TOO_LARGE -10   /* grid exceeds the fixed scratch of smadft_r2r3d_noalloc */
 
 /* ---- models, precisions, fields -------------------------------------------------------- */
 #define SMADFT_MODEL_NOADV 0  /* no-adv/cosNoAdvTrackSing.cpp */
@@ -173,6 +174,24 @@ int smadft_r2r_pass_device(smadft_ctx *ctx, const void *in, void *out, int axis,
  * 3 RODFT01 per axis; in may equal out; both 16-byte aligned.  precision SMADFT_FP64 (double*) or SMADFT_FP32
  * (float*).  Uses the context's stream and scratch field; the context's grid must match. */
 int smadft_r2r3d_device(smadft_ctx *ctx, const void *in, void *out, int kx, int ky, int kz);
+
+/* The same 3-D r2r transform for callers that cannot allocate device memory.  No
+ * counterpart in the reference: FFTW plans own their buffers there.  Some callers cannot
+ * call cudaMalloc -- code in a stream callback or cudaLaunchHostFunc host function, code
+ * whose device memory is fully reserved by another allocator, or fixed-latency loops where
+ * cudaMalloc's implicit device synchronisation is not acceptable.  This entry point needs
+ * no context and allocates nothing: the intermediate field lives in a fixed file-scope
+ * device array of SMADFT_NOALLOC_MAX_BYTES that every GPU loading the library holds until
+ * exit.  Limits: nx*ny*nz*element_size <= SMADFT_NOALLOC_MAX_BYTES (else
+ * SMADFT_ERR_TOO_LARGE), lengths even, <= 512, factors 2, 3, 5.  in/out 16-byte aligned
+ * device buffers (double* for SMADFT_FP64, float* for SMADFT_FP32); in may equal out.  The
+ * work is queued on `stream` (a cudaStream_t, NULL = legacy default stream).  All calls
+ * share the array, so calls that overlap on the GPU race; a call needs nothing from earlier
+ * calls (it writes every scratch element before reading it).  The first call on a device
+ * looks the array up for that device and should come before any stream capture. */
+#define SMADFT_NOALLOC_MAX_BYTES (16u << 20)
+int smadft_r2r3d_noalloc(const void *in, void *out, int nx, int ny, int nz, int kx, int ky, int kz,
+                         int precision, void *stream);
 
 /* ---- initial-condition builders (host only, no device) --------------------------------
  * All write nx*ny*nz doubles in the reference layout; grid spacing dx = 2 pi/(q0 nw). */

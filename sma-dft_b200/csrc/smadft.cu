@@ -348,6 +348,7 @@ const char *smadft_error_string(int code)
     case SMADFT_ERR_IO: return "checkpoint I/O error";
     case SMADFT_ERR_STATE: return "call out of order";
     case SMADFT_ERR_NODEVICE: return "no CUDA device";
+    case SMADFT_ERR_TOO_LARGE: return "grid exceeds the no-alloc scratch maximum";
     default: return "unknown error";
     }
 }

@@ -25,7 +25,9 @@ REDFT10, REDFT01, RODFT10, RODFT01 = 0, 1, 2, 3
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory",
           -4: "non-finite field", -5: "device wait timed out", -6: "unsupported grid length",
-          -7: "checkpoint I/O error", -8: "call out of order", -9: "no CUDA device"}
+          -7: "checkpoint I/O error", -8: "call out of order", -9: "no CUDA device",
+          -10: "grid exceeds the no-alloc scratch maximum"}
+NOALLOC_MAX_BYTES = 16 << 20
 
 
 class SmadftError(RuntimeError):
@@ -87,6 +89,8 @@ SIGNATURES = [
     ("smadft_step_host", ctypes.c_int, [_vp, _dp, ctypes.c_size_t, ctypes.c_int]),
     ("smadft_get_stream", ctypes.c_int, [_vp, _P(_vp)]),
     ("smadft_launch_count", ctypes.c_int, [_vp, _P(ctypes.c_longlong)]),
+    ("smadft_r2r3d_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     ("smadft_ic_interface", ctypes.c_int, [_P(Params), ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_ulonglong, _dp]),
     ("smadft_ic_focal_conic", ctypes.c_int, [_P(Params), ctypes.c_double, ctypes.c_double, _dp]),
@@ -159,6 +163,13 @@ def ic_conics(p: Params, A=0.5, count=4, rmin=3.0, rmax=6.0, noise=1e-3, seed=20
     out = np.empty((p.nx, p.ny, p.nz), dtype=np.float64)
     _check(lib().smadft_ic_conics(ctypes.byref(p), A, count, rmin, rmax, noise, seed, _dptr(out)))
     return out
+
+
+def r2r3d_noalloc(src_ptr: int, dst_ptr: int, shape, kinds, precision: int = FP64, stream: int = 0) -> int:
+    """smadft_r2r3d_noalloc on device pointers; returns the status code (0 = ok)."""
+    nx, ny, nz = (int(s) for s in shape)
+    return int(lib().smadft_r2r3d_noalloc(_vp(src_ptr), _vp(dst_ptr), nx, ny, nz,
+                                          *[int(k) for k in kinds], int(precision), _vp(stream)))
 
 
 class Solver:
