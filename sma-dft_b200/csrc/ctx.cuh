@@ -7,10 +7,12 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <type_traits>
 #include <string>
 #include <vector>
 
 #include "r2r_fast.cuh"
+#include "r2r_rd.cuh"
 #include "r2r_pass.cuh"
 #include "smadft.h"
 
@@ -74,6 +76,7 @@ struct Ctx {
     bool psi_current = false;   // adv: S_PSI holds iCT(psihat) of the current state
     long long launches = 0;     // kernels launched by this context
     bool use_fast = true;       // compile-time-length pass kernels where available
+    bool use_rd = true;         // register-direct kernels for plain strided passes
     double *stage = nullptr;    // FP64 staging field for host-psi steps (allocated on first use)
 
     template <typename T>
@@ -152,11 +155,36 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
+template <typename T, int N, int AXIS, class ST>
+int launch_rd(Ctx &c, int kind, const T *src, ST st)
+{
+    const PlanDev &pd = c.plans.at(N);
+    const int tiles_b = (c.g.nz + 31) / 32;
+    const long long tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b;
+    constexpr size_t smem = rd_smem_bytes<T, N>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, ST>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    r2r_rd_kernel<T, N, AXIS, ST><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+        c.g, kind, tiles_b, src, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
+    SMADFT_CUDA(cudaGetLastError());
+    c.launches++;
+    return SMADFT_OK;
+}
+
+// z passes run more CTAs per SM (fewer registers); strided passes keep two
+template <int AXIS>
+using FastCfgFor = typename std::conditional<AXIS == 2, FastCfg<32, 256, 4, 3>, FastDefault>::type;
+
 template <typename T, int N, int AXIS, class LD, class ST>
 int launch_fast(Ctx &c, int kind, LD ld, ST st)
 {
+    using CFG = FastCfgFor<AXIS>;
     const PlanDev &pd = c.plans.at(N);
-    const int W = kFastW;
+    const int W = CFG::W;
     int tiles_b = 1;
     long long tiles;
     if (AXIS == 2) {
@@ -165,14 +193,14 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
         tiles_b = (c.g.nz + W - 1) / W;
         tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b;
     }
-    constexpr size_t smem = fast_smem_bytes<T, N>();
+    constexpr size_t smem = fast_smem_bytes<T, N, CFG>();
     static bool attr_set = false;
     if (!attr_set) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_fast_kernel<T, N, AXIS, LD, ST>,
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_fast_kernel<T, N, AXIS, LD, ST, CFG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
-    r2r_fast_kernel<T, N, AXIS, LD, ST><<<(unsigned)tiles, kFastThreads, smem, c.stream>>>(
+    r2r_fast_kernel<T, N, AXIS, LD, ST, CFG><<<(unsigned)tiles, CFG::THREADS, smem, c.stream>>>(
         c.g, kind, tiles_b, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), ld, st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
@@ -186,6 +214,16 @@ template <typename T, int AXIS, class LD, class ST>
 int launch_axis(Ctx &c, int kind, LD ld, ST st)
 {
     const int n = AXIS == 0 ? c.g.nx : (AXIS == 1 ? c.g.ny : c.g.nz);
+    if constexpr (AXIS != 2 && std::is_same<LD, LoadArr<T>>::value) {
+        if (c.use_rd) {
+            switch (n) {
+            case 64: return launch_rd<T, 64, AXIS>(c, kind, ld.p, st);
+            case 128: return launch_rd<T, 128, AXIS>(c, kind, ld.p, st);
+            case 256: return launch_rd<T, 256, AXIS>(c, kind, ld.p, st);
+            default: break;
+            }
+        }
+    }
     if (c.use_fast) {
         switch (n) {
 #define SMADFT_CASE(N_) \

@@ -248,19 +248,29 @@ __device__ __forceinline__ ElemPos tile_elem(const Geom &g, const TileBase &tb, 
     return e;
 }
 
-constexpr int kFastW = 32;        // real lines per tile
-constexpr int kFastThreads = 256;
+// Launch shape of the pass kernel: W real lines per tile, THREADS per CTA, at most MAXB
+// 16-byte loads in flight per thread, MINB CTAs per SM for the register budget.
+template <int W_, int THREADS_, int MAXB_, int MINB_>
+struct FastCfg {
+    static constexpr int W = W_;
+    static constexpr int THREADS = THREADS_;
+    static constexpr int MAXB = MAXB_;
+    static constexpr int MINB = MINB_;
+};
+using FastDefault = FastCfg<32, 256, 8, 2>;
+constexpr int kFastW = FastDefault::W;        // real lines per tile
+constexpr int kFastThreads = FastDefault::THREADS;
 
-// largest divisor of `per` not above 8
-constexpr int batch_size(int per)
+// largest divisor of `per` not above `maxb`
+constexpr int batch_size(int per, int maxb = 8)
 {
-    for (int b = 8; b > 1; b--)
+    for (int b = maxb; b > 1; b--)
         if (per % b == 0) return b;
     return 1;
 }
 
-template <typename T, int N>
-constexpr size_t fast_smem_bytes() { return ((size_t)(kFastW / 2) * PlanInfo<N>::LD + 2 * N) * sizeof(cpx<T>); }
+template <typename T, int N, class CFG = FastDefault>
+constexpr size_t fast_smem_bytes() { return ((size_t)(CFG::W / 2) * PlanInfo<N>::LD + 2 * N) * sizeof(cpx<T>); }
 
 // Post-twiddle of a forward (DCT-II) transform: output for line part `odd` (0 = real line A,
 // 1 = real line B) from Z[k] and Z[N-k] of the packed complex line (see fft_tile.cuh).
@@ -270,16 +280,17 @@ __device__ __forceinline__ T dct2_out(cpx<T> zk, cpx<T> zm, cpx<T> hh, int odd)
     return odd ? hh.x * (zk.y + zm.y) - hh.y * (zk.x - zm.x) : hh.x * (zk.x + zm.x) + hh.y * (zk.y - zm.y);
 }
 
-template <typename T, int N, int AXIS, class LD, class ST>
-__global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int kind, int tiles_b,
-                                                                   const cpx<T> *__restrict__ wt_g,
-                                                                   const cpx<T> *__restrict__ ht_g, LD ld, ST st)
+template <typename T, int N, int AXIS, class LD, class ST, class CFG = FastDefault>
+__global__ void __launch_bounds__(CFG::THREADS, CFG::MINB) r2r_fast_kernel(Geom g, int kind, int tiles_b,
+                                                                           const cpx<T> *__restrict__ wt_g,
+                                                                           const cpx<T> *__restrict__ ht_g, LD ld, ST st)
 {
     using PI = PlanInfo<N>;
-    constexpr int W = kFastW, NL = W / 2;
+    constexpr int W = CFG::W, NL = W / 2;
+    constexpr int NT = CFG::THREADS;
     constexpr int V = 16 / sizeof(T);             // elements per 16-byte global access
-    constexpr int PERV = N * W / V / kFastThreads; // vector accesses per thread
-    constexpr int BATCH = batch_size(PERV);
+    constexpr int PERV = N * W / V / NT;          // vector accesses per thread
+    constexpr int BATCH = batch_size(PERV, CFG::MAXB);
     static_assert(PERV % BATCH == 0, "tile must split evenly");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T> *buf = reinterpret_cast<cpx<T> *>(smem_raw);
@@ -291,7 +302,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int k
     const bool sine = (kind == K_DST2 || kind == K_DST3);
     // 16-byte accesses need V | nz (element index alignment); otherwise V = 1 accesses
     const bool vec_ok = (g.nz % V) == 0;
-    for (int m = threadIdx.x; m < N; m += kFastThreads) {
+    for (int m = threadIdx.x; m < N; m += NT) {
         wt[m] = wt_g[m];
         ht[m] = ht_g[m];
     }
@@ -305,7 +316,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int k
         int tt[BATCH], ww[BATCH];
 #pragma unroll
         for (int b = 0; b < BATCH; b++) {
-            const int e = (e0 + b) * kFastThreads + threadIdx.x;
+            const int e = (e0 + b) * NT + threadIdx.x;
             int t, w;
             if (AXIS == 2) { t = (e % (N / V)) * V; w = e / (N / V); }
             else { w = (e % (W / V)) * V; t = e / (W / V); }
@@ -352,7 +363,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int k
         // DCT-III pre-twiddle, in place on pairs (t, N - t): Z_t = V_A[t] + i V_B[t],
         // V[t] = exp(+i pi t / 2N) (X_t - i X_{N-t}), X_N = 0
         constexpr int HALF = N / 2 + 1;
-        for (int e = threadIdx.x; e < NL * HALF; e += kFastThreads) {
+        for (int e = threadIdx.x; e < NL * HALF; e += NT) {
             const int c = e / HALF;
             const int t = e - c * HALF;
             cpx<T> *L = buf + c * PI::LD;
@@ -380,7 +391,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) r2r_fast_kernel(Geom g, int k
     }
 
     // ---- shared -> global, output permutation / post-twiddle per kind
-    for (int e = threadIdx.x; e < N * W / V; e += kFastThreads) {
+    for (int e = threadIdx.x; e < N * W / V; e += NT) {
         int o, w;
         if (AXIS == 2) { o = (e % (N / V)) * V; w = e / (N / V); }
         else { w = (e % (W / V)) * V; o = e / (W / V); }

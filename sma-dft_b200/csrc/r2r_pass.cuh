@@ -66,7 +66,7 @@ __device__ __forceinline__ ElemPos elem_pos(const PassArgs<T> &a, int t, int w)
 }
 
 // V consecutive elements p[idx .. idx+V-1]; for V > 1, idx is a multiple of V and p is
-// 16-byte aligned (one 16-byte access: float4 / double2).
+// 16-byte aligned (one 8- or 16-byte access: float2 / float4 / double2).
 template <typename T, int V>
 __device__ __forceinline__ void vld(const T *__restrict__ p, long long idx, T *o)
 {
@@ -75,6 +75,9 @@ __device__ __forceinline__ void vld(const T *__restrict__ p, long long idx, T *o
         o[0] = u.x; o[1] = u.y; o[2] = u.z; o[3] = u.w;
     } else if constexpr (V == 2 && sizeof(T) == 8) {
         const double2 u = *reinterpret_cast<const double2 *>(p + idx);
+        o[0] = u.x; o[1] = u.y;
+    } else if constexpr (V == 2 && sizeof(T) == 4) {
+        const float2 u = *reinterpret_cast<const float2 *>(p + idx);
         o[0] = u.x; o[1] = u.y;
     } else {
 #pragma unroll
@@ -89,6 +92,8 @@ __device__ __forceinline__ void vst(T *__restrict__ p, long long idx, const T *v
         *reinterpret_cast<float4 *>(p + idx) = make_float4(v[0], v[1], v[2], v[3]);
     } else if constexpr (V == 2 && sizeof(T) == 8) {
         *reinterpret_cast<double2 *>(p + idx) = make_double2(v[0], v[1]);
+    } else if constexpr (V == 2 && sizeof(T) == 4) {
+        *reinterpret_cast<float2 *>(p + idx) = make_float2(v[0], v[1]);
     } else {
 #pragma unroll
         for (int q = 0; q < V; q++) p[idx + q] = v[q];
