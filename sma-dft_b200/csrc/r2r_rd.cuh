@@ -12,7 +12,9 @@
 // (LoadArr); passes that compute their input from several fields use r2r_fast_kernel.
 //
 // Index conventions follow r2r_fast.cuh: DIF stage 0 (radix R0, stride R1) then stage 1
-// (radix R1, stride 1); position b*R1 + q then holds X[b + R0 q].
+// (radix R1, stride 1); position b*R1 + q then holds X[b + R0 q].  The pairings X[p] /
+// X[N-p] (DCT-III pre-twiddle) and X[k] / X[N-k] (DCT-II post-twiddle) are done with one
+// warp shuffle per value: butterflies j and R1 - j sit in the two halves of one warp.
 #pragma once
 
 #include "r2r_fast.cuh"
@@ -61,8 +63,13 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2
         wt[m] = wt_g[m];
         ht[m] = ht_g[m];
     }
-    const int c = threadIdx.x % kRdLines;
-    const int j = threadIdx.x / kRdLines;
+    // Thread (c, j): c = complex line (fastest, for coalescing), j = first-stage butterfly.
+    // Warp w holds the butterfly pair {j, R1 - j} (warp 0: {0, R1/2}) in its two half-warps:
+    // X[N - p] for the points p of butterfly j lives in butterfly R1 - j (lane ^ 16), and the
+    // same pairing holds for X[k] / X[N - k] after the last stage.
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5, hh16 = lane >> 4;
+    const int c = lane & 15;
+    const int j = (wi == 0) ? (hh16 ? R1 / 2 : 0) : (hh16 ? R1 - wi : wi);
     // tile: 32 k-columns starting at k0 along the non-transformed line coordinate `a`
     const int kt = blockIdx.x % tiles_b;
     const int a = blockIdx.x / tiles_b;
@@ -84,6 +91,22 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2
         }
         return {nk == 1 ? src[q] : T(0), T(0)};
     };
+    // partner values: out[q] = x of the point N - p(q) (see the pairing above)
+    auto partner = [&](const cpx<T> *x, cpx<T> *out, int jj) {
+        if (wi == 0) {
+#pragma unroll
+            for (int q = 0; q < R0; q++) {
+                if (jj == 0) out[q] = (q == 0) ? cpx<T>{T(0), T(0)} : x[(R0 - q) % R0];
+                else out[q] = x[R0 - 1 - q];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < R0; q++) {
+                out[q].x = __shfl_xor_sync(0xffffffffu, x[R0 - 1 - q].x, 16);
+                out[q].y = __shfl_xor_sync(0xffffffffu, x[R0 - 1 - q].y, 16);
+            }
+        }
+    };
 
     cpx<T> v[R0];
     if (fwd) {
@@ -98,16 +121,21 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2
         }
     } else {
         // DCT-III pre-twiddle Z_p = V_A[p] + i V_B[p], V[p] = exp(+i pi p/2N)(X_p - i X_{N-p}),
-        // X_N = 0; DST-III reads the line reversed
+        // X_N = 0; DST-III reads the line reversed.  X_{N-p} comes from the partner lane.
+        cpx<T> xa[R0], xb[R0];
 #pragma unroll
         for (int q = 0; q < R0; q++) {
             const int p = j + q * R1;
-            const cpx<T> xa = load_pair(sine ? N - 1 - p : p);
-            const cpx<T> xb = (p == 0) ? cpx<T>{T(0), T(0)} : load_pair(sine ? p - 1 : N - p);
+            xa[q] = load_pair(sine ? N - 1 - p : p);
+        }
+        partner(xa, xb, j);
+#pragma unroll
+        for (int q = 0; q < R0; q++) {
+            const int p = j + q * R1;
             const cpx<T> hh = ht[p];
             const T cc = hh.x, ss = hh.y;
-            const T var = cc * xa.x + ss * xb.x, vai = ss * xa.x - cc * xb.x;
-            const T vbr = cc * xa.y + ss * xb.y, vbi = ss * xa.y - cc * xb.y;
+            const T var = cc * xa[q].x + ss * xb[q].x, vai = ss * xa[q].x - cc * xb[q].x;
+            const T vbr = cc * xa[q].y + ss * xb[q].y, vbi = ss * xa[q].y - cc * xb[q].y;
             v[q] = {var - vbi, vai + vbr};
         }
     }
@@ -164,28 +192,56 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2
         }
         return;
     }
-    // forward: DCT-II post-twiddle pairs X[k] with X[N-k]; exchange through shared memory
-    // (each thread rewrites only its own blocks, so no barrier is needed before this)
+    // forward: DCT-II post-twiddle pairs X[k] with X[N-k].  With one block per thread the
+    // partner is lane ^ 16 (or the thread itself in warp 0); otherwise through shared memory.
+    if constexpr (BPT == 1) {
+        // block b = j holds X[j + R0 q]; N - (j + R0 q) = (R1... ) is block R1 - j, q' = R1 - 1 - q
+        // for j != 0 (R0 == R1 here), and block 0, q' = R1 - q for j == 0
+        cpx<T> xm[R1];
+        if (wi == 0) {
 #pragma unroll
-    for (int r = 0; r < BPT; r++) {
-        const int b = j + r * R1;
-        cpx<T> *pb = line + RI::phys(b * R1);
+            for (int q = 0; q < R1; q++) {
+                if (j == 0) xm[q] = x1[0][(R1 - q) % R1];
+                else xm[q] = x1[0][R1 - 1 - q];
+            }
+        } else {
 #pragma unroll
-        for (int q = 0; q < R1; q++) pb[q] = x1[r][q];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < BPT; r++) {
-        const int b = j + r * R1;
+            for (int q = 0; q < R1; q++) {
+                xm[q].x = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].x, 16);
+                xm[q].y = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].y, 16);
+            }
+        }
 #pragma unroll
         for (int q = 0; q < R1; q++) {
-            const int kk = b + R0 * q;
-            const int km = kk == 0 ? 0 : N - kk;
-            const cpx<T> zk = x1[r][q];
-            const cpx<T> zm = line[RI::phys((km % R0) * R1 + km / R0)];
+            const int kk = j + R0 * q;
+            const cpx<T> zk = x1[0][q];
             const cpx<T> hh = ht[kk];
-            const T A = dct2_out(zk, zm, hh, 0), B = dct2_out(zk, zm, hh, 1);
+            const T A = dct2_out(zk, xm[q], hh, 0), B = dct2_out(zk, xm[q], hh, 1);
             store_pair(sine ? N - 1 - kk : kk, A, B);
+        }
+    } else {
+        // each thread rewrites only its own blocks, so no barrier is needed before this
+#pragma unroll
+        for (int r = 0; r < BPT; r++) {
+            const int b = j + r * R1;
+            cpx<T> *pb = line + RI::phys(b * R1);
+#pragma unroll
+            for (int q = 0; q < R1; q++) pb[q] = x1[r][q];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < BPT; r++) {
+            const int b = j + r * R1;
+#pragma unroll
+            for (int q = 0; q < R1; q++) {
+                const int kk = b + R0 * q;
+                const int km = kk == 0 ? 0 : N - kk;
+                const cpx<T> zk = x1[r][q];
+                const cpx<T> zm = line[RI::phys((km % R0) * R1 + km / R0)];
+                const cpx<T> hh = ht[kk];
+                const T A = dct2_out(zk, zm, hh, 0), B = dct2_out(zk, zm, hh, 1);
+                store_pair(sine ? N - 1 - kk : kk, A, B);
+            }
         }
     }
 }
