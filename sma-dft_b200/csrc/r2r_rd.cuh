@@ -48,7 +48,7 @@ template <int N>
 __device__ __forceinline__ int makhoul_src(int p) { return p < N / 2 ? 2 * p : 2 * (N - 1 - p) + 1; }
 
 template <typename T, int N, int AXIS, class ST>
-__global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2r_rd_kernel(Geom g, int kind, int tiles_b,
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, int kind, int tiles_b,
                                                                        const T *__restrict__ src,
                                                                        const cpx<T> *__restrict__ wt_g,
                                                                        const cpx<T> *__restrict__ ht_g, ST st)
@@ -91,23 +91,6 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2
         }
         return {nk == 1 ? src[q] : T(0), T(0)};
     };
-    // partner values: out[q] = x of the point N - p(q) (see the pairing above)
-    auto partner = [&](const cpx<T> *x, cpx<T> *out, int jj) {
-        if (wi == 0) {
-#pragma unroll
-            for (int q = 0; q < R0; q++) {
-                if (jj == 0) out[q] = (q == 0) ? cpx<T>{T(0), T(0)} : x[(R0 - q) % R0];
-                else out[q] = x[R0 - 1 - q];
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < R0; q++) {
-                out[q].x = __shfl_xor_sync(0xffffffffu, x[R0 - 1 - q].x, 16);
-                out[q].y = __shfl_xor_sync(0xffffffffu, x[R0 - 1 - q].y, 16);
-            }
-        }
-    };
-
     cpx<T> v[R0];
     if (fwd) {
         // stage-0 points p = j + q R1 of the Makhoul-permuted sequence
@@ -121,22 +104,51 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2
         }
     } else {
         // DCT-III pre-twiddle Z_p = V_A[p] + i V_B[p], V[p] = exp(+i pi p/2N)(X_p - i X_{N-p}),
-        // X_N = 0; DST-III reads the line reversed.  X_{N-p} comes from the partner lane.
-        cpx<T> xa[R0], xb[R0];
+        // X_N = 0; DST-III reads the line reversed.  X_{N-p} comes from the partner lane (or
+        // the thread itself in warp 0); each pair of points is rewritten in place together so
+        // only one array stays live.
 #pragma unroll
         for (int q = 0; q < R0; q++) {
             const int p = j + q * R1;
-            xa[q] = load_pair(sine ? N - 1 - p : p);
+            v[q] = load_pair(sine ? N - 1 - p : p);
         }
-        partner(xa, xb, j);
-#pragma unroll
-        for (int q = 0; q < R0; q++) {
-            const int p = j + q * R1;
-            const cpx<T> hh = ht[p];
+        auto ztw = [&](int q, cpx<T> xa, cpx<T> xb) -> cpx<T> {
+            const cpx<T> hh = ht[j + q * R1];
             const T cc = hh.x, ss = hh.y;
-            const T var = cc * xa[q].x + ss * xb[q].x, vai = ss * xa[q].x - cc * xb[q].x;
-            const T vbr = cc * xa[q].y + ss * xb[q].y, vbi = ss * xa[q].y - cc * xb[q].y;
-            v[q] = {var - vbi, vai + vbr};
+            const T var = cc * xa.x + ss * xb.x, vai = ss * xa.x - cc * xb.x;
+            const T vbr = cc * xa.y + ss * xb.y, vbi = ss * xa.y - cc * xb.y;
+            return {var - vbi, vai + vbr};
+        };
+        if (wi != 0 || j == R1 / 2) {
+            // partner point of q is R0 - 1 - q (in lane ^ 16, or here for j = R1/2)
+#pragma unroll
+            for (int q = 0; q < R0 / 2; q++) {
+                const int qb = R0 - 1 - q;
+                cpx<T> pa, pb;
+                if (wi != 0) {
+                    pa.x = __shfl_xor_sync(0xffffffffu, v[qb].x, 16);
+                    pa.y = __shfl_xor_sync(0xffffffffu, v[qb].y, 16);
+                    pb.x = __shfl_xor_sync(0xffffffffu, v[q].x, 16);
+                    pb.y = __shfl_xor_sync(0xffffffffu, v[q].y, 16);
+                } else {
+                    pa = v[qb];
+                    pb = v[q];
+                }
+                const cpx<T> za = ztw(q, v[q], pa), zb = ztw(qb, v[qb], pb);
+                v[q] = za;
+                v[qb] = zb;
+            }
+        } else {
+            // j = 0: partner of q is R0 - q (q = 0 pairs with X_N = 0, q = R0/2 with itself)
+            v[0] = ztw(0, v[0], cpx<T>{T(0), T(0)});
+            v[R0 / 2] = ztw(R0 / 2, v[R0 / 2], v[R0 / 2]);
+#pragma unroll
+            for (int q = 1; q < R0 / 2; q++) {
+                const int qb = R0 - q;
+                const cpx<T> za = ztw(q, v[q], v[qb]), zb = ztw(qb, v[qb], v[q]);
+                v[q] = za;
+                v[qb] = zb;
+            }
         }
     }
 
@@ -195,29 +207,28 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 8 ? 1 : 2) r2
     // forward: DCT-II post-twiddle pairs X[k] with X[N-k].  With one block per thread the
     // partner is lane ^ 16 (or the thread itself in warp 0); otherwise through shared memory.
     if constexpr (BPT == 1) {
-        // block b = j holds X[j + R0 q]; N - (j + R0 q) = (R1... ) is block R1 - j, q' = R1 - 1 - q
-        // for j != 0 (R0 == R1 here), and block 0, q' = R1 - q for j == 0
-        cpx<T> xm[R1];
-        if (wi == 0) {
-#pragma unroll
-            for (int q = 0; q < R1; q++) {
-                if (j == 0) xm[q] = x1[0][(R1 - q) % R1];
-                else xm[q] = x1[0][R1 - 1 - q];
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < R1; q++) {
-                xm[q].x = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].x, 16);
-                xm[q].y = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].y, 16);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < R1; q++) {
+        // block j holds X[j + R0 q]; X[N - k] is block R1 - j at q' = R1 - 1 - q (lane ^ 16, or
+        // this thread for j = R1/2), and block 0 at q' = (R1 - q) mod R1 for j = 0
+        auto emit = [&](int q, cpx<T> zm) {
             const int kk = j + R0 * q;
             const cpx<T> zk = x1[0][q];
             const cpx<T> hh = ht[kk];
-            const T A = dct2_out(zk, xm[q], hh, 0), B = dct2_out(zk, xm[q], hh, 1);
-            store_pair(sine ? N - 1 - kk : kk, A, B);
+            store_pair(sine ? N - 1 - kk : kk, dct2_out(zk, zm, hh, 0), dct2_out(zk, zm, hh, 1));
+        };
+        if (wi != 0) {
+#pragma unroll
+            for (int q = 0; q < R1; q++) {
+                cpx<T> zm;
+                zm.x = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].x, 16);
+                zm.y = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].y, 16);
+                emit(q, zm);
+            }
+        } else if (j == R1 / 2) {
+#pragma unroll
+            for (int q = 0; q < R1; q++) emit(q, x1[0][R1 - 1 - q]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < R1; q++) emit(q, x1[0][(R1 - q) % R1]);
         }
     } else {
         // each thread rewrites only its own blocks, so no barrier is needed before this
