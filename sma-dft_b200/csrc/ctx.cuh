@@ -155,8 +155,8 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
-template <typename T, int N, int AXIS, class ST>
-int launch_rd(Ctx &c, int kind, const T *src, ST st)
+template <typename T, int N, int AXIS, class LD, class ST>
+int launch_rd(Ctx &c, int kind, LD ld, ST st)
 {
     const PlanDev &pd = c.plans.at(N);
     const int tiles_b = (c.g.nz + 31) / 32;
@@ -164,12 +164,12 @@ int launch_rd(Ctx &c, int kind, const T *src, ST st)
     constexpr size_t smem = rd_smem_bytes<T, N>();
     static bool attr_set = false;
     if (!attr_set) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, ST>,
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
-    r2r_rd_kernel<T, N, AXIS, ST><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
-        c.g, kind, tiles_b, src, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
+    r2r_rd_kernel<T, N, AXIS, LD, ST><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+        c.g, kind, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
     return SMADFT_OK;
@@ -207,31 +207,40 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
-// Line lengths with a compile-time kernel (the configs' grids); others use the generic one.
+// Line lengths with a compile-time staged kernel (the configs' grids); others use the
+// generic one.  Strided axes of length 64/128/256 run the register-direct kernel instead.
 #define SMADFT_FAST_SIZES(X) X(64) X(96) X(128) X(160) X(256)
+#define SMADFT_FAST_SIZES_STRIDED(X) X(96) X(160)
 
 template <typename T, int AXIS, class LD, class ST>
 int launch_axis(Ctx &c, int kind, LD ld, ST st)
 {
     const int n = AXIS == 0 ? c.g.nx : (AXIS == 1 ? c.g.ny : c.g.nz);
-    if constexpr (AXIS != 2 && std::is_same<LD, LoadArr<T>>::value) {
+    if constexpr (AXIS != 2) {
         if (c.use_rd) {
             switch (n) {
-            case 64: return launch_rd<T, 64, AXIS>(c, kind, ld.p, st);
-            case 128: return launch_rd<T, 128, AXIS>(c, kind, ld.p, st);
-            case 256: return launch_rd<T, 256, AXIS>(c, kind, ld.p, st);
+            case 64: return launch_rd<T, 64, AXIS>(c, kind, ld, st);
+            case 128: return launch_rd<T, 128, AXIS>(c, kind, ld, st);
+            case 256: return launch_rd<T, 256, AXIS>(c, kind, ld, st);
             default: break;
             }
         }
     }
     if (c.use_fast) {
-        switch (n) {
 #define SMADFT_CASE(N_) \
     case N_: return launch_fast<T, N_, AXIS>(c, kind, ld, st);
-            SMADFT_FAST_SIZES(SMADFT_CASE)
-#undef SMADFT_CASE
-        default: break;
+        if constexpr (AXIS == 2) {
+            switch (n) {
+                SMADFT_FAST_SIZES(SMADFT_CASE)
+            default: break;
+            }
+        } else {
+            switch (n) {
+                SMADFT_FAST_SIZES_STRIDED(SMADFT_CASE)
+            default: break;
+            }
         }
+#undef SMADFT_CASE
     }
     return launch_generic<T>(c, AXIS, kind, ld, st);
 }
@@ -261,15 +270,16 @@ int convert(Ctx &c, const S *src, D *dst)
     return SMADFT_OK;
 }
 
-// 3-D transform: z pass (custom loader) -> y pass -> x pass (custom storer), in place on
-// the scratch field.
+// 3-D transform: y pass (custom loader) -> z pass -> x pass (custom storer), in place on
+// the scratch field.  The fused loader and storer run in the register-direct strided
+// kernels; the z pass in between only moves the scratch field.
 template <typename T, class LD, class ST>
 int r2r3d(Ctx &c, int kx, int ky, int kz, LD ld, ST st)
 {
     T *tmp = c.f<T>(S_TMP);
-    int rc = launch_axis<T, 2>(c, kz, ld, StoreArr<T>{tmp});
+    int rc = launch_axis<T, 1>(c, ky, ld, StoreArr<T>{tmp});
     if (rc) return rc;
-    rc = launch_axis<T, 1>(c, ky, LoadArr<T>{tmp}, StoreArr<T>{tmp});
+    rc = launch_axis<T, 2>(c, kz, LoadArr<T>{tmp}, StoreArr<T>{tmp});
     if (rc) return rc;
     return launch_axis<T, 0>(c, kx, LoadArr<T>{tmp}, st);
 }

@@ -8,8 +8,8 @@
 // contiguous bytes -- so the tile is never staged in shared memory on the way in.  Shared
 // memory carries only the one exchange between the two radix stages (and, for the forward
 // kinds, the X[k] / X[N-k] pairing of the DCT-II post-twiddle).  Outputs go straight from
-// registers to global memory through the Storer.  The input is always a plain array
-// (LoadArr); passes that compute their input from several fields use r2r_fast_kernel.
+// registers to global memory through the Storer, and inputs come through the Loader, so
+// the fused multi-field loaders and storers of the model steps run here too.
 //
 // Index conventions follow r2r_fast.cuh: DIF stage 0 (radix R0, stride R1) then stage 1
 // (radix R1, stride 1); position b*R1 + q then holds X[b + R0 q].  The pairings X[p] /
@@ -47,9 +47,8 @@ constexpr size_t rd_smem_bytes() { return ((size_t)kRdLines * RdInfo<N>::LD + 2 
 template <int N>
 __device__ __forceinline__ int makhoul_src(int p) { return p < N / 2 ? 2 * p : 2 * (N - 1 - p) + 1; }
 
-template <typename T, int N, int AXIS, class ST>
-__global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, int kind, int tiles_b,
-                                                                       const T *__restrict__ src,
+template <typename T, int N, int AXIS, class LD, class ST>
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, int kind, int tiles_b, LD ld,
                                                                        const cpx<T> *__restrict__ wt_g,
                                                                        const cpx<T> *__restrict__ ht_g, ST st)
 {
@@ -81,15 +80,15 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, i
     const bool sine = (kind == K_DST2 || kind == K_DST3);
     __syncthreads();
 
-    // the pair of real samples (lines k, k+1) at line position t, packed as one complex
+    // the pair of real samples (lines k, k+1) at line position t, packed as one complex;
+    // the Loader computes them from its fields (each point is loaded exactly once)
     auto load_pair = [&](int t) -> cpx<T> {
         const long long q = base + (long long)t * stride;
-        if (nk >= 2) {
-            T v[2];
-            vld<T, 2>(src, q, v);
-            return {v[0], v[1]};
-        }
-        return {nk == 1 ? src[q] : T(0), T(0)};
+        const int ii = AXIS == 1 ? a : t, jj = AXIS == 1 ? t : a;
+        T v[2] = {T(0), T(0)};
+        if (nk >= 2) ld.template load<2>(q, ii, jj, k, v);
+        else if (nk == 1) ld.template load<1>(q, ii, jj, k, v);
+        return {v[0], v[1]};
     };
     cpx<T> v[R0];
     if (fwd) {

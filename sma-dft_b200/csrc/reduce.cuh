@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(kRedThreads) reduce_partials(long long n, F f,
     }
 }
 
-__global__ void reduce_final(const double *partials, int nblocks, double *out)
+static __global__ void reduce_final(const double *partials, int nblocks, double *out)
 {
     // one warp per value, fixed order
     const int v = threadIdx.x >> 5, lane = threadIdx.x & 31;

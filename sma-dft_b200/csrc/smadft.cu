@@ -11,10 +11,9 @@
 #include <vector>
 
 #include "ctx.cuh"
-#include "models.cuh"
-#include "quasi.cuh"
 #include "reduce.cuh"
 #include "smadft.h"
+#include "steps.h"
 
 using namespace smadft;
 
@@ -122,70 +121,6 @@ std::vector<int> slots_for(int model)
     return s;
 }
 
-// ---------------------------------------------------------------- steps ---------------
-template <typename T>
-int noadv_step(Ctx &c, bool keep_old)
-{
-    Spec<T> s = make_spec<T>(c);
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
-    // N^n = REDFT10^3(beta psi^3 - gamma psi^5), fused CN/AB2 update of psihat
-    int rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
-                      StUpdCN<T>{s, ph, np});
-    if (rc) return rc;
-    // psi^{n+1} = REDFT01^3 psihat (into the second buffer when the old psi is needed)
-    T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
-    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{dst});
-}
-
-template <typename T>
-int adv_step(Ctx &c)
-{
-    Spec<T> s = make_spec<T>(c);
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
-    T *gx = c.f<T>(S_GX), *gy = c.f<T>(S_GY), *gz = c.f<T>(S_GZ), *sp2 = c.f<T>(S_SP2);
-    T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
-    T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
-    int rc;
-    // psi and grad psi from psihat (adv/cosAdvTrackMult.cpp:904-975)
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{psi}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdGrad<T, 0>{s, ph}, StoreArr<T>{gx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdGrad<T, 1>{s, ph}, StoreArr<T>{gy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdGrad<T, 2>{s, ph}, StoreArr<T>{gz}))) return rc;
-    // Sp2 = iCT(-L psihat) (:980-991)
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdNegLin<T>{s, ph}, StoreArr<T>{sp2}))) return rc;
-    // force spectra S_c = ST_c(mu d_c psi) (:996-1027)
-    if ((rc = r2r3d<T>(c, K_DST2, K_DCT2, K_DCT2, LdForce<T>{psi, sp2, gx, s.beta, s.gamma}, StoreArr<T>{Sx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DST2, K_DCT2, LdForce<T>{psi, sp2, gy, s.beta, s.gamma}, StoreArr<T>{Sy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DST2, LdForce<T>{psi, sp2, gz, s.beta, s.gamma}, StoreArr<T>{Sz}))) return rc;
-    // Stokes velocity (:1030-1286)
-    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vz}))) return rc;
-    // N = beta psi^3 - gamma psi^5 - v.grad psi, CN/AB2 update (:1290-1365)
-    return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
-                    LdAdvN<T>{psi, vx, vy, vz, gx, gy, gz, s.beta, s.gamma}, StUpdCN<T>{s, ph, np});
-}
-
-template <typename T>
-int refresh_psi(Ctx &c, T *dst)
-{
-    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{c.f<T>(S_PSIH)}, StoreArr<T>{dst});
-}
-
-template <typename T>
-int pre_loop(Ctx &c)
-{
-    Spec<T> s = make_spec<T>(c);
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
-    int rc;
-    if (c.p.model == SMADFT_MODEL_QUASI) return quasi_pre_loop<T>(c);
-    // psihat = scale REDFT10^3 psi ; Nprev = REDFT10^3(beta psi^3 - gamma psi^5) (no advection)
-    // no-adv/cosNoAdvTrackSing.cpp:618-635, adv/cosAdvTrackMult.cpp:760-777
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, s.scale}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma}, StoreArr<T>{np}))) return rc;
-    return SMADFT_OK;
-}
-
 // Graph variant of the next loop body (see StepGraph).
 int step_variant(const Ctx &c)
 {
@@ -260,10 +195,9 @@ int free_energy_t(Ctx &c, double *out)
 {
     int rc;
     if ((rc = ensure_psi<T>(c))) return rc;
-    Spec<T> s = make_spec<T>(c);
     T *fp = c.f<T>(S_PSI2);
     // f' = REDFT01^3(alpha (q0^2 - q^2) psihat)  (quasi/quasi.cpp:1121-1137)
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdDfd<T>{s, c.f<T>(S_PSIH)}, StoreArr<T>{fp}))) return rc;
+    if ((rc = dfd_field<T>(c, fp))) return rc;
     double e;
     if ((rc = reduce_energy<T>(c, c.f<T>(S_PSI), fp, &e))) return rc;
     *out = e * c.dx * c.dx * c.dx;
@@ -299,12 +233,11 @@ int step_host_t(Ctx &c, double *host, int nsteps)
 {
     if (!c.stage) SMADFT_CUDA(cudaMalloc(&c.stage, sizeof(double) * c.n));
     SMADFT_CUDA(cudaMemcpyAsync(c.stage, host, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream));
-    Spec<T> s = make_spec<T>(c);
     T *psi = c.f<T>(S_PSI);
     int rc;
     // psi from the host; psihat = scale REDFT10^3 psi (the reference's per-step planPsi)
     if ((rc = convert<double, T>(c, c.stage, psi))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{c.f<T>(S_PSIH), s.scale}))) return rc;
+    if ((rc = psihat_from_psi<T>(c))) return rc;
     c.psi_current = true;
     for (int q = 0; q < nsteps; q++) {
         if ((rc = one_step<T>(c, false))) return rc;
@@ -630,9 +563,8 @@ int smadft_r2r_pass_device(smadft_ctx *h, const void *in, void *out, int axis, i
     if (((uintptr_t)in | (uintptr_t)out) & 15) return fail(h->c, SMADFT_ERR_INVALID, "buffers must be 16-byte aligned");
     Ctx &c = h->c;
     cudaSetDevice(c.dev);
-    if (c.f32)
-        return launch_pass<float>(c, axis, kind, LoadArr<float>{(const float *)in}, StoreArr<float>{(float *)out});
-    return launch_pass<double>(c, axis, kind, LoadArr<double>{(const double *)in}, StoreArr<double>{(double *)out});
+    if (c.f32) return plain_pass<float>(c, (const float *)in, (float *)out, axis, kind);
+    return plain_pass<double>(c, (const double *)in, (double *)out, axis, kind);
 }
 
 int smadft_r2r3d_device(smadft_ctx *h, const void *in, void *out, int kx, int ky, int kz)
@@ -643,9 +575,8 @@ int smadft_r2r3d_device(smadft_ctx *h, const void *in, void *out, int kx, int ky
     Ctx &c = h->c;
     if (((uintptr_t)in | (uintptr_t)out) & 15) return fail(c, SMADFT_ERR_INVALID, "buffers must be 16-byte aligned");
     cudaSetDevice(c.dev);
-    if (c.f32)
-        return r2r3d<float>(c, kx, ky, kz, LoadArr<float>{(const float *)in}, StoreArr<float>{(float *)out});
-    return r2r3d<double>(c, kx, ky, kz, LoadArr<double>{(const double *)in}, StoreArr<double>{(double *)out});
+    if (c.f32) return plain_r2r3d<float>(c, (const float *)in, (float *)out, kx, ky, kz);
+    return plain_r2r3d<double>(c, (const double *)in, (double *)out, kx, ky, kz);
 }
 
 }  // extern "C"

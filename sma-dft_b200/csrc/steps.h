@@ -1,0 +1,29 @@
+// steps.h -- the per-model loop bodies and transform helpers, compiled in separate
+// translation units (step_*.cu) and instantiated for float and double.
+#pragma once
+
+#include "ctx.cuh"
+
+namespace smadft {
+
+// no-adv/cosNoAdvTrackSing.cpp:681-764,1072 (keep_old: psi^{n+1} into S_PSI2)
+template <typename T> int noadv_step(Ctx &c, bool keep_old);
+// adv/cosAdvTrackMult.cpp:824-1369,1742
+template <typename T> int adv_step(Ctx &c);
+// quasi/quasi.cpp:1099-2190 (nloop = 1-based step counter)
+template <typename T> int quasi_step(Ctx &c, long long nloop, bool keep_old);
+// pre-loop blocks: no-adv :618-635, adv :760-777, quasi :990-1062
+template <typename T> int pre_loop(Ctx &c);
+// psi = REDFT01^3 psihat into dst
+template <typename T> int refresh_psi(Ctx &c, T *dst);
+// f' = REDFT01^3(alpha (q0^2 - q^2) psihat) into dst (quasi/quasi.cpp:1121-1137)
+template <typename T> int dfd_field(Ctx &c, T *dst);
+// psihat = scale REDFT10^3 psi (the reference's per-step planPsi, host-psi steps)
+template <typename T> int psihat_from_psi(Ctx &c);
+// plain transforms on caller buffers
+template <typename T> int plain_r2r3d(Ctx &c, const T *in, T *out, int kx, int ky, int kz);
+template <typename T> int plain_pass(Ctx &c, const T *in, T *out, int axis, int kind);
+// quasi diagnostics sums: ms[0] = sum rho, ms[1] = sum e
+template <typename T> int reduce_mass_energy(Ctx &c, double *ms);
+
+}  // namespace smadft
