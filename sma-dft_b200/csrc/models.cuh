@@ -226,20 +226,32 @@ struct StUpdCN {
     Spec<T> s;
     T *__restrict__ ph;
     T *__restrict__ np;
+    static constexpr int PRE = 2;   // psihat, Nprev
     template <int V>
-    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    __device__ __forceinline__ void pre(long long q, int, int, int, T *buf) const
     {
-        T p[V], n0[V], o[V];
-        vld<T, V>(ph, q, p);
-        vld<T, V>(np, q, n0);
+        vld<T, V>(ph, q, buf);
+        vld<T, V>(np, q, buf + V);
+    }
+    template <int V>
+    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *buf) const
+    {
+        T o[V];
 #pragma unroll
         for (int u = 0; u < V; u++) {
             const T al = s.alin(i, j, k + u);
             const T c1 = T(1) + s.dtd2 * al, c2 = T(1) - s.dtd2 * al;
-            o[u] = (c1 * p[u] + s.dtd2 * s.scale * (T(3) * v[u] - n0[u])) / c2;
+            o[u] = (c1 * buf[u] + s.dtd2 * s.scale * (T(3) * v[u] - buf[V + u])) / c2;
         }
         vst<T, V>(ph, q, o);
         vst<T, V>(np, q, v);
+    }
+    template <int V>
+    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    {
+        T buf[2 * V];
+        pre<V>(q, i, j, k, buf);
+        fin<V>(q, i, j, k, v, buf);
     }
 };
 
@@ -248,6 +260,14 @@ template <typename T>
 struct StScale {
     T *__restrict__ p;
     T scale;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *) const
+    {
+        store<V>(q, i, j, k, v);
+    }
     template <int V>
     __device__ __forceinline__ void store(long long q, int, int, int, const T *v) const
     {

@@ -63,6 +63,14 @@ template <typename T>
 struct StFilter {
     Spec<T> s;
     T *__restrict__ out;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *) const
+    {
+        store<V>(q, i, j, k, v);
+    }
     template <int V>
     __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
@@ -113,6 +121,14 @@ template <typename T>
 struct StLapSpec {
     Spec<T> s;
     T *__restrict__ out;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *) const
+    {
+        store<V>(q, i, j, k, v);
+    }
     template <int V>
     __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
@@ -214,23 +230,35 @@ struct StUpdBDF {
     Spec<T> s;
     T *__restrict__ ph, *__restrict__ pho, *__restrict__ np;
     int first;
+    static constexpr int PRE = 3;   // psihat, psihat_old, Nprev
     template <int V>
-    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    __device__ __forceinline__ void pre(long long q, int, int, int, T *buf) const
     {
-        T old[V], oo[V], n0[V], o[V];
-        vld<T, V>(ph, q, old);
-        vld<T, V>(pho, q, oo);
-        vld<T, V>(np, q, n0);
+        vld<T, V>(ph, q, buf);
+        vld<T, V>(pho, q, buf + V);
+        vld<T, V>(np, q, buf + 2 * V);
+    }
+    template <int V>
+    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *buf) const
+    {
+        T o[V];
 #pragma unroll
         for (int u = 0; u < V; u++) {
             const T al = s.alin(i, j, k + u);
             const T c1 = T(2) - s.dt * s.rho_m * al, c2 = T(1.5) - s.dt * s.rho_m * al;
-            const T npv = first ? v[u] : n0[u];
-            o[u] = (c1 * old[u] - T(0.5) * oo[u] + s.dtd2 * s.scale * (T(3) * v[u] - npv)) / c2;
+            const T npv = first ? v[u] : buf[2 * V + u];
+            o[u] = (c1 * buf[u] - T(0.5) * buf[V + u] + s.dtd2 * s.scale * (T(3) * v[u] - npv)) / c2;
         }
         vst<T, V>(ph, q, o);
-        vst<T, V>(pho, q, old);
+        vst<T, V>(pho, q, buf);
         vst<T, V>(np, q, v);
+    }
+    template <int V>
+    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    {
+        T buf[3 * V];
+        pre<V>(q, i, j, k, buf);
+        fin<V>(q, i, j, k, v, buf);
     }
 };
 

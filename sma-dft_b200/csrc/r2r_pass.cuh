@@ -102,7 +102,10 @@ __device__ __forceinline__ void vst(T *__restrict__ p, long long idx, const T *v
 
 // Functor interface of the pass kernels.  A loader fills out[0..V-1] with the transform
 // input at (i, j, k+u), u < V (memory idx+u, consecutive along z); a storer consumes the
-// transform output for the same V elements.
+// transform output for the same V elements.  A storer that reads state before writing it
+// (the spectral updates) exposes the read as pre() (PRE values per element into buf) and
+// the rest as fin(), so kernels can issue the reads of several elements before any write;
+// store() = pre() + fin().
 template <typename T>
 struct LoadArr {
     const T *__restrict__ p;
@@ -112,9 +115,18 @@ struct LoadArr {
 template <typename T>
 struct StoreArr {
     T *__restrict__ p;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void fin(long long idx, int, int, int, const T *v, const T *) const { vst<T, V>(p, idx, v); }
     template <int V>
     __device__ __forceinline__ void store(long long idx, int, int, int, const T *v) const { vst<T, V>(p, idx, v); }
 };
+
+// buffer length for a storer's pre() values of V elements (at least 1)
+template <class ST, int V>
+constexpr int pre_len() { return ST::PRE * V > 0 ? ST::PRE * V : 1; }
 
 template <typename T, class LD, class ST>
 __global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST st)

@@ -54,6 +54,8 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, i
 {
     using RI = RdInfo<N>;
     constexpr int R0 = RI::R0, R1 = RI::R1, NT = RI::THREADS;
+    constexpr int BPT = R0 / R1 > 0 ? R0 / R1 : 1;   // last-stage blocks per thread
+    constexpr int NP = BPT * R1;                      // output points per thread (= R0)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T> *buf = reinterpret_cast<cpx<T> *>(smem_raw);
     cpx<T> *wt = buf + kRdLines * RI::LD;
@@ -69,48 +71,54 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, i
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5, hh16 = lane >> 4;
     const int c = lane & 15;
     const int j = (wi == 0) ? (hh16 ? R1 / 2 : 0) : (hh16 ? R1 - wi : wi);
-    // tile: 32 k-columns starting at k0 along the non-transformed line coordinate `a`
+    // tile: 32 k-columns starting at kt*32 along the non-transformed line coordinate `a`
     const int kt = blockIdx.x % tiles_b;
     const int a = blockIdx.x / tiles_b;
     const int k = kt * 32 + 2 * c;                 // first of the two real lines
     const long long stride = AXIS == 1 ? (long long)g.nz : g.nyz;
     const long long base = (AXIS == 1 ? (long long)a * g.nyz : (long long)a * g.nz) + k;
     const int nk = g.nz - k;                       // real lines of this pair inside the box
+    const bool full = (kt + 1) * 32 <= g.nz;       // CTA-uniform: no line outside the box
     const bool fwd = (kind == K_DCT2 || kind == K_DST2);
     const bool sine = (kind == K_DST2 || kind == K_DST3);
     __syncthreads();
 
     // the pair of real samples (lines k, k+1) at line position t, packed as one complex;
     // the Loader computes them from its fields (each point is loaded exactly once)
-    auto load_pair = [&](int t) -> cpx<T> {
+    auto load_pair = [&](int t, bool edge) -> cpx<T> {
         const long long q = base + (long long)t * stride;
         const int ii = AXIS == 1 ? a : t, jj = AXIS == 1 ? t : a;
         T v[2] = {T(0), T(0)};
-        if (nk >= 2) ld.template load<2>(q, ii, jj, k, v);
+        if (!edge || nk >= 2) ld.template load<2>(q, ii, jj, k, v);
         else if (nk == 1) ld.template load<1>(q, ii, jj, k, v);
         return {v[0], v[1]};
     };
+    auto src_pos = [&](int q) -> int {       // natural line position of stage-0 point q
+        const int p = j + q * R1;
+        if (fwd) return makhoul_src<N>(p);
+        return sine ? N - 1 - p : p;
+    };
+
     cpx<T> v[R0];
-    if (fwd) {
-        // stage-0 points p = j + q R1 of the Makhoul-permuted sequence
+    if (full) {
 #pragma unroll
-        for (int q = 0; q < R0; q++) {
-            const int p = j + q * R1;
-            const int t = makhoul_src<N>(p);
-            cpx<T> x = load_pair(t);
-            if (sine && (t & 1)) x = {-x.x, -x.y};
-            v[q] = x;
+        for (int q = 0; q < R0; q++) v[q] = load_pair(src_pos(q), false);
+    } else {
+#pragma unroll
+        for (int q = 0; q < R0; q++) v[q] = load_pair(src_pos(q), true);
+    }
+    if (fwd) {
+        // Makhoul-permuted input: DST-II negates odd natural samples
+        if (sine) {
+#pragma unroll
+            for (int q = 0; q < R0; q++)
+                if (src_pos(q) & 1) v[q] = {-v[q].x, -v[q].y};
         }
     } else {
         // DCT-III pre-twiddle Z_p = V_A[p] + i V_B[p], V[p] = exp(+i pi p/2N)(X_p - i X_{N-p}),
         // X_N = 0; DST-III reads the line reversed.  X_{N-p} comes from the partner lane (or
         // the thread itself in warp 0); each pair of points is rewritten in place together so
         // only one array stays live.
-#pragma unroll
-        for (int q = 0; q < R0; q++) {
-            const int p = j + q * R1;
-            v[q] = load_pair(sine ? N - 1 - p : p);
-        }
         auto ztw = [&](int q, cpx<T> xa, cpx<T> xb) -> cpx<T> {
             const cpx<T> hh = ht[j + q * R1];
             const T cc = hh.x, ss = hh.y;
@@ -164,7 +172,6 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, i
     __syncthreads();
 
     // ---- stage 1: radix R1 over contiguous blocks; block b holds X[b + R0 q] afterwards
-    constexpr int BPT = R0 / R1 > 0 ? R0 / R1 : 1;   // blocks per thread
     cpx<T> x1[BPT][R1];
 #pragma unroll
     for (int r = 0; r < BPT; r++) {
@@ -176,82 +183,118 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, i
         else codelet<R1, T, true>(x1[r]);
     }
 
-    auto store_pair = [&](int o, T A, T B) {
-        const long long q = base + (long long)o * stride;
-        const int ii = AXIS == 1 ? a : o, jj = AXIS == 1 ? o : a;
-        if (nk >= 2) {
-            const T w2[2] = {A, B};
-            st.template store<2>(q, ii, jj, k, w2);
-        } else if (nk == 1) {
-            st.template store<1>(q, ii, jj, k, &A);
-        }
+    // ---- outputs: (real line A, real line B) pairs in x1; line position of point pnt
+    auto out_row = [&](int pnt) -> int {
+        const int kk = j + (pnt / R1) * R1 + R0 * (pnt % R1);   // X index held by point pnt
+        if (fwd) return sine ? N - 1 - kk : kk;
+        return kk < N / 2 ? 2 * kk : 2 * (N - 1 - kk) + 1;
     };
-
     if (!fwd) {
         // DCT-III output y[2m] = v[m], y[2m+1] = v[N-1-m]; DST-III negates odd outputs
 #pragma unroll
-        for (int r = 0; r < BPT; r++) {
-            const int b = j + r * R1;
+        for (int r = 0; r < BPT; r++)
 #pragma unroll
             for (int q = 0; q < R1; q++) {
-                const int m = b + R0 * q;
+                const int m = j + r * R1 + R0 * q;
                 const int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
-                cpx<T> z = x1[r][q];
-                if (sine && (o & 1)) z = {-z.x, -z.y};
-                store_pair(o, z.x, z.y);
+                if (sine && (o & 1)) x1[r][q] = {-x1[r][q].x, -x1[r][q].y};
             }
-        }
-        return;
-    }
-    // forward: DCT-II post-twiddle pairs X[k] with X[N-k].  With one block per thread the
-    // partner is lane ^ 16 (or the thread itself in warp 0); otherwise through shared memory.
-    if constexpr (BPT == 1) {
-        // block j holds X[j + R0 q]; X[N - k] is block R1 - j at q' = R1 - 1 - q (lane ^ 16, or
-        // this thread for j = R1/2), and block 0 at q' = (R1 - q) mod R1 for j = 0
-        auto emit = [&](int q, cpx<T> zm) {
-            const int kk = j + R0 * q;
-            const cpx<T> zk = x1[0][q];
-            const cpx<T> hh = ht[kk];
-            store_pair(sine ? N - 1 - kk : kk, dct2_out(zk, zm, hh, 0), dct2_out(zk, zm, hh, 1));
-        };
-        if (wi != 0) {
+    } else {
+        // DCT-II post-twiddle pairs X[k] with X[N-k]
+        if constexpr (BPT == 1) {
+            // X[N - k] is block R1 - j at q' = R1 - 1 - q (lane ^ 16, or this thread for
+            // j = R1/2), or block 0 at q' = (R1 - q) mod R1 for j = 0; each pair (q, q') is
+            // rewritten in place together
+            auto post = [&](int q, cpx<T> zm) -> cpx<T> {
+                const int kk = j + R0 * q;
+                const cpx<T> hh = ht[kk];
+                return {dct2_out(x1[0][q], zm, hh, 0), dct2_out(x1[0][q], zm, hh, 1)};
+            };
+            if (wi != 0 || j == R1 / 2) {
 #pragma unroll
-            for (int q = 0; q < R1; q++) {
-                cpx<T> zm;
-                zm.x = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].x, 16);
-                zm.y = __shfl_xor_sync(0xffffffffu, x1[0][R1 - 1 - q].y, 16);
-                emit(q, zm);
+                for (int q = 0; q < R1 / 2; q++) {
+                    const int qb = R1 - 1 - q;
+                    cpx<T> pa, pb;
+                    if (wi != 0) {
+                        pa.x = __shfl_xor_sync(0xffffffffu, x1[0][qb].x, 16);
+                        pa.y = __shfl_xor_sync(0xffffffffu, x1[0][qb].y, 16);
+                        pb.x = __shfl_xor_sync(0xffffffffu, x1[0][q].x, 16);
+                        pb.y = __shfl_xor_sync(0xffffffffu, x1[0][q].y, 16);
+                    } else {
+                        pa = x1[0][qb];
+                        pb = x1[0][q];
+                    }
+                    const cpx<T> oa = post(q, pa), ob = post(qb, pb);
+                    x1[0][q] = oa;
+                    x1[0][qb] = ob;
+                }
+            } else {
+                const cpx<T> o0 = post(0, x1[0][0]);
+                const cpx<T> oh = post(R1 / 2, x1[0][R1 / 2]);
+#pragma unroll
+                for (int q = 1; q < R1 / 2; q++) {
+                    const int qb = R1 - q;
+                    const cpx<T> oa = post(q, x1[0][qb]), ob = post(qb, x1[0][q]);
+                    x1[0][q] = oa;
+                    x1[0][qb] = ob;
+                }
+                x1[0][0] = o0;
+                x1[0][R1 / 2] = oh;
             }
-        } else if (j == R1 / 2) {
-#pragma unroll
-            for (int q = 0; q < R1; q++) emit(q, x1[0][R1 - 1 - q]);
         } else {
+            // through shared memory (each thread rewrites only its own blocks first)
 #pragma unroll
-            for (int q = 0; q < R1; q++) emit(q, x1[0][(R1 - q) % R1]);
+            for (int r = 0; r < BPT; r++) {
+                cpx<T> *pb = line + RI::phys((j + r * R1) * R1);
+#pragma unroll
+                for (int q = 0; q < R1; q++) pb[q] = x1[r][q];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < BPT; r++)
+#pragma unroll
+                for (int q = 0; q < R1; q++) {
+                    const int kk = j + r * R1 + R0 * q;
+                    const int km = kk == 0 ? 0 : N - kk;
+                    const cpx<T> zm = line[RI::phys((km % R0) * R1 + km / R0)];
+                    const cpx<T> hh = ht[kk];
+                    const cpx<T> zk = x1[r][q];
+                    x1[r][q] = {dct2_out(zk, zm, hh, 0), dct2_out(zk, zm, hh, 1)};
+                }
+        }
+    }
+
+    // ---- stores: the storer's reads (pre) for a chunk of points go out before its writes
+    constexpr int CH = 4;
+    constexpr int PL = pre_len<ST, 2>();
+    auto put = [&](int pnt, bool edge, const T *pre_buf) {
+        const cpx<T> z = x1[pnt / R1][pnt % R1];
+        const int o = out_row(pnt);
+        const long long q = base + (long long)o * stride;
+        const int ii = AXIS == 1 ? a : o, jj = AXIS == 1 ? o : a;
+        const T w2[2] = {z.x, z.y};
+        if (!edge || nk >= 2) st.template fin<2>(q, ii, jj, k, w2, pre_buf);
+        else if (nk == 1) st.template store<1>(q, ii, jj, k, w2);
+    };
+    if (full) {
+#pragma unroll
+        for (int p0 = 0; p0 < NP; p0 += CH) {
+            T pre_buf[CH][PL];
+#pragma unroll
+            for (int u = 0; u < CH; u++) {
+                const int o = out_row(p0 + u);
+                st.template pre<2>(base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < CH; u++) put(p0 + u, false, pre_buf[u]);
         }
     } else {
-        // each thread rewrites only its own blocks, so no barrier is needed before this
 #pragma unroll
-        for (int r = 0; r < BPT; r++) {
-            const int b = j + r * R1;
-            cpx<T> *pb = line + RI::phys(b * R1);
-#pragma unroll
-            for (int q = 0; q < R1; q++) pb[q] = x1[r][q];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < BPT; r++) {
-            const int b = j + r * R1;
-#pragma unroll
-            for (int q = 0; q < R1; q++) {
-                const int kk = b + R0 * q;
-                const int km = kk == 0 ? 0 : N - kk;
-                const cpx<T> zk = x1[r][q];
-                const cpx<T> zm = line[RI::phys((km % R0) * R1 + km / R0)];
-                const cpx<T> hh = ht[kk];
-                const T A = dct2_out(zk, zm, hh, 0), B = dct2_out(zk, zm, hh, 1);
-                store_pair(sine ? N - 1 - kk : kk, A, B);
-            }
+        for (int p0 = 0; p0 < NP; p0++) {
+            T pre_buf[PL];
+            const int o = out_row(p0);
+            if (nk >= 2) st.template pre<2>(base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
+            put(p0, true, pre_buf);
         }
     }
 }
