@@ -41,7 +41,8 @@ struct LdNonlin {
 };
 
 // Index-shifted gradient spectra (adv/cosAdvTrackMult.cpp:904-959): G_c = -s_c f[+1 along c],
-// zero at the last index of c.
+// zero at the last index of c.  Branch-free: out-of-range points read a clamped in-range
+// address and are zeroed by a select, so the loads of all points can be issued together.
 template <typename T, int AX>
 struct LdGrad {
     Spec<T> s;
@@ -51,19 +52,19 @@ struct LdGrad {
     {
         if (AX == 0 || AX == 1) {
             const bool in = AX == 0 ? (i < s.nx - 1) : (j < s.ny - 1);
-            if (!in) {
-#pragma unroll
-                for (int u = 0; u < V; u++) out[u] = T(0);
-                return;
-            }
+            const long long sh = AX == 0 ? s.nyz : (long long)s.nz;
             T v[V];
-            vld<T, V>(f, q + (AX == 0 ? s.nyz : (long long)s.nz), v);
-            const T sc = AX == 0 ? s.sx[i] : s.sy[j];
+            vld<T, V>(f, in ? q + sh : q, v);
+            const T sc = in ? -(AX == 0 ? s.sx[i] : s.sy[j]) : T(0);
 #pragma unroll
-            for (int u = 0; u < V; u++) out[u] = -sc * v[u];
+            for (int u = 0; u < V; u++) out[u] = sc * v[u];
         } else {
 #pragma unroll
-            for (int u = 0; u < V; u++) out[u] = (k + u < s.nz - 1) ? -s.sz[k + u] * f[q + u + 1] : T(0);
+            for (int u = 0; u < V; u++) {
+                const bool in = k + u < s.nz - 1;
+                const T x = f[in ? q + u + 1 : q + u];
+                out[u] = in ? -s.sz[k + u] * x : T(0);
+            }
         }
     }
 };
@@ -111,24 +112,19 @@ template <typename T, int AX, bool DIVV>
 struct LdStokes {
     Spec<T> s;
     const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz, *__restrict__ dv;
+    // Branch-free: neighbours outside the box read a clamped in-range address and are
+    // zeroed by selects; truncated modes are zeroed at the end.
     template <int V>
     __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
         const T snu = s.scale / s.nu;
         if (AX == 0) {
-            if (i >= s.nx - 1) {
-#pragma unroll
-                for (int u = 0; u < V; u++) out[u] = T(0);
-                return;
-            }
-            const long long qn = q + s.nyz;   // (i+1, j, k)
+            const bool live = i < s.nx - 1;
+            const long long qn = live ? q + s.nyz : q;         // (i+1, j, k)
+            const bool jy = j != 0;
             T sx[V], sy[V], d[V];
             vld<T, V>(Sx, q, sx);
-            if (j != 0) vld<T, V>(Sy, qn - s.nz, sy);
-            else {
-#pragma unroll
-                for (int u = 0; u < V; u++) sy[u] = T(0);
-            }
+            vld<T, V>(Sy, jy ? qn - s.nz : qn, sy);             // (i+1, j-1, k)
             if (DIVV) vld<T, V>(dv, qn, d);
             const T si = s.sx[i], qj = s.qy[j];
             const T a2 = si * si + qj * qj;
@@ -136,47 +132,41 @@ struct LdStokes {
             for (int u = 0; u < V; u++) {
                 const int kk = k + u;
                 const T qk = s.qz[kk];
-                const T sz = (kk != 0) ? Sz[qn - 1 + u] : T(0);
+                const bool kz = kk != 0;
+                const T szr = Sz[kz ? qn - 1 + u : qn + u];       // (i+1, j, k-1)
+                const T syv = jy ? sy[u] : T(0), sz = kz ? szr : T(0);
                 const T inv = T(1) / (a2 + qk * qk);
-                const T dot = si * sx[u] + qj * sy[u] + qk * sz;
+                const T dot = si * sx[u] + qj * syv + qk * sz;
                 T v = snu * inv * (sx[u] - si * inv * dot);
                 if (DIVV) v = v + snu * inv * (s.nu * si * d[u]);
-                out[u] = v;
+                out[u] = live ? v : T(0);
             }
         } else if (AX == 1) {
-            if (j >= s.ny - 1) {
-#pragma unroll
-                for (int u = 0; u < V; u++) out[u] = T(0);
-                return;
-            }
+            const bool live = j < s.ny - 1;
+            const long long qj1 = live ? q + s.nz : q;          // (i, j+1, k)
+            const bool ix = i != 0;
             T syv[V], sx[V], d[V];
             vld<T, V>(Sy, q, syv);
-            if (i != 0) vld<T, V>(Sx, q - s.nyz + s.nz, sx);              // (i-1, j+1, k)
-            else {
-#pragma unroll
-                for (int u = 0; u < V; u++) sx[u] = T(0);
-            }
-            if (DIVV) vld<T, V>(dv, q + s.nz, d);
+            vld<T, V>(Sx, ix ? qj1 - s.nyz : qj1, sx);          // (i-1, j+1, k)
+            if (DIVV) vld<T, V>(dv, qj1, d);
             const T qi = s.qx[i], sj = s.sy[j];
             const T a2 = qi * qi + sj * sj;
 #pragma unroll
             for (int u = 0; u < V; u++) {
                 const int kk = k + u;
-                if (kk >= s.nz - 1) { out[u] = T(0); continue; }
                 const T qk = s.qz[kk];
-                const T sz = (kk != 0) ? Sz[q + s.nz - 1 + u] : T(0);      // (i, j+1, k-1)
+                const bool kz = kk != 0;
+                const T szr = Sz[kz ? qj1 - 1 + u : qj1 + u];     // (i, j+1, k-1)
+                const T sxv = ix ? sx[u] : T(0), sz = kz ? szr : T(0);
                 const T inv = T(1) / (a2 + qk * qk);
-                const T dot = qi * sx[u] + sj * syv[u] + qk * sz;
+                const T dot = qi * sxv + sj * syv[u] + qk * sz;
                 T v = snu * inv * (syv[u] - sj * inv * dot);
                 if (DIVV) v = v + snu * inv * (s.nu * sj * d[u]);
-                out[u] = v;
+                out[u] = (live && kk < s.nz - 1) ? v : T(0);
             }
         } else {
-            if (j >= s.ny - 1) {
-#pragma unroll
-                for (int u = 0; u < V; u++) out[u] = T(0);
-                return;
-            }
+            const bool live = j < s.ny - 1;
+            const bool ix = i != 0, jy = j != 0;
             T szv[V];
             vld<T, V>(Sz, q, szv);
             const T qi = s.qx[i], qj = s.qy[j];
@@ -184,15 +174,17 @@ struct LdStokes {
 #pragma unroll
             for (int u = 0; u < V; u++) {
                 const int kk = k + u;
-                if (kk >= s.nz - 1) { out[u] = T(0); continue; }
+                const bool kl = kk < s.nz - 1;
+                const long long qk1 = kl ? q + 1 + u : q + u;    // (i, j, k+1)
                 const T sk = s.sz[kk];
-                const T sx = (i != 0) ? Sx[q - s.nyz + 1 + u] : T(0);      // (i-1, j, k+1)
-                const T sy = (j != 0) ? Sy[q - s.nz + 1 + u] : T(0);       // (i, j-1, k+1)
+                const T sxr = Sx[ix ? qk1 - s.nyz : qk1];         // (i-1, j, k+1)
+                const T syr = Sy[jy ? qk1 - s.nz : qk1];          // (i, j-1, k+1)
+                const T sx = ix ? sxr : T(0), sy = jy ? syr : T(0);
                 const T inv = T(1) / (a2 + sk * sk);
                 const T dot = qi * sx + qj * sy + sk * szv[u];
                 T v = snu * inv * (szv[u] - sk * inv * dot);
-                if (DIVV) v = v + snu * inv * (s.nu * sk * dv[q + 1 + u]);
-                out[u] = v;
+                if (DIVV) v = v + snu * inv * (s.nu * sk * dv[qk1]);
+                out[u] = (live && kl) ? v : T(0);
             }
         }
     }

@@ -179,16 +179,20 @@ struct LdPressure {
     template <int V>
     __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
+        // branch-free: missing neighbours read a clamped address and are zeroed by selects
 #pragma unroll
         for (int u = 0; u < V; u++) {
             const int kk = k + u;
             const long long qq = q + u;
-            if (i + j + kk == 0) { out[u] = T(0); continue; }
-            const T sx = (i > 0) ? Sx[qq - s.nyz] : T(0);
-            const T sy = (j > 0) ? Sy[qq - s.nz] : T(0);
-            const T sz = (kk > 0) ? Sz[qq - 1] : T(0);
-            out[u] = s.scale * (-(s.qx[i] * sx + s.qy[j] * sy + s.qz[kk] * sz) / s.mq2(i, j, kk) +
-                                (s.lam + T(2) * s.nu) * dv[qq]);
+            const T sxr = Sx[i > 0 ? qq - s.nyz : qq];
+            const T syr = Sy[j > 0 ? qq - s.nz : qq];
+            const T szr = Sz[kk > 0 ? qq - 1 : qq];
+            const T sx = i > 0 ? sxr : T(0), sy = j > 0 ? syr : T(0), sz = kk > 0 ? szr : T(0);
+            const bool origin = (i + j + kk) == 0;
+            const T m2 = origin ? T(1) : s.mq2(i, j, kk);
+            const T v = s.scale * (-(s.qx[i] * sx + s.qy[j] * sy + s.qz[kk] * sz) / m2 +
+                                   (s.lam + T(2) * s.nu) * dv[qq]);
+            out[u] = origin ? T(0) : v;
         }
     }
 };
