@@ -49,7 +49,12 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 50 ms.
+
+    ``start()`` waits (up to 10 s) until the first sample has arrived, so that the sampler is
+    running before the timed region begins; ``mark(t0, t1)`` keeps the samples that arrived
+    inside the timed region (host wall clock).
+    """
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -58,25 +63,33 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
+        self.window = (0.0, float("inf"))
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0: float, t1: float):
+        self.window = (t0, t1)
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -86,7 +99,10 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lo, hi = self.window
+        for ts, ln in self.lines:
+            if not (lo <= ts <= hi):
+                continue
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -99,7 +115,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "interval_ms": 50}
 
 
 def cpu_reference_run(steps: int, psi0: np.ndarray | None, threads: int):
@@ -152,7 +168,7 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
-def timed_steps(torch, solver, steps: int, dist, world):
+def timed_steps(torch, solver, steps: int, dist, world, sampler=None):
     """Device time of `steps` loop bodies on the solver's stream, max over ranks."""
     stream = torch.cuda.ExternalStream(solver.stream)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -160,10 +176,13 @@ def timed_steps(torch, solver, steps: int, dist, world):
         dist.barrier()
     torch.cuda.synchronize()
     l0 = solver.launches
+    t0 = time.time()
     ev0.record(stream)
     solver.step(steps)
     ev1.record(stream)
     torch.cuda.synchronize()
+    if sampler is not None:
+        sampler.mark(t0, time.time())
     ms = ev0.elapsed_time(ev1)
     launches = solver.launches - l0
     if world > 1:
@@ -174,29 +193,50 @@ def timed_steps(torch, solver, steps: int, dist, world):
     return ms, launches
 
 
+def profile_traffic(name: str):
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        with open(path) as f:
+            m = re.search(r"traffic_per_launch_bytes\s*=\s*([0-9]+)", f.read())
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
 def pass_roofline(torch, smadft, peak):
-    """Per-launch time of the strided (y-axis) DCT-II pass on a 256^3 FP32 field."""
+    """Average launch time of the plain DCT-II pass along each axis of a 256^3 FP32 field.
+
+    The passes run through a ring of 6 fields (384 MiB, well above the 126 MB L2): launch r
+    reads field r mod 6 and writes field r+1 mod 6, so every launch reads a field that was
+    last written five launches earlier.  Algorithmic bytes per launch = one field read + one
+    field written = 2 x 4 B x 256^3.
+    """
+    ring = 6
     p = smadft.params(smadft.ADV, (N, N, N), precision=smadft.FP32, **CFG)
     with smadft.Solver(p) as s:
-        x = torch.randn((N, N, N), device="cuda", dtype=torch.float32)
-        y = torch.empty_like(x)
+        bufs = [torch.randn((N, N, N), device="cuda", dtype=torch.float32) for _ in range(ring)]
         torch.cuda.synchronize()
         stream = torch.cuda.ExternalStream(s.stream)
         out = {}
         for axis, name in ((2, "z"), (1, "y"), (0, "x")):
-            for _ in range(3):
-                s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, 0)
-            reps = 20
+            for r in range(ring):
+                s.r2r_pass_device(bufs[r].data_ptr(), bufs[(r + 1) % ring].data_ptr(), axis, 0)
+            reps = 10 * ring
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             ev0.record(stream)
-            for _ in range(reps):
-                s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, 0)
+            for r in range(reps):
+                s.r2r_pass_device(bufs[r % ring].data_ptr(), bufs[(r + 1) % ring].data_ptr(), axis, 0)
             ev1.record(stream)
             torch.cuda.synchronize()
             us = 1000.0 * ev0.elapsed_time(ev1) / reps
             gbs = 2.0 * 4 * N ** 3 / (us * 1e-6) / 1e9
             out[name] = {"us": us, "gbs": gbs, "frac": gbs / peak}
+            # refill: repeated unnormalised DCT-II passes grow the values by about 2N each
+            for bft in bufs:
+                bft.normal_()
+            torch.cuda.synchronize()
         return out
 
 
@@ -224,7 +264,7 @@ def run_ours(args, rank, world, local_rank):
             s.sync()
             if name == "fp32":
                 with ClockSampler(local_rank) as cs:
-                    ms, launches = timed_steps(torch, s, args.steps, dist, world)
+                    ms, launches = timed_steps(torch, s, args.steps, dist, world, cs)
                 clocks = cs.summary()
                 launches_fp32 = launches
             else:
@@ -270,20 +310,14 @@ def run_ours(args, rank, world, local_rank):
         return 0
 
     algo_bytes = 4.0 * N ** 3 * F_ADV
-    achieved = algo_bytes / (ms_step * 1e-3) / 1e9
+    achieved_step = algo_bytes / (ms_step * 1e-3) / 1e9
     cpu = {}
     try:
-        sps, secs, kind, sample = cpu_reference_run(2, psi0, os.cpu_count() or 1)
+        sps, secs, kind, sample = cpu_reference_run(4, psi0, os.cpu_count() or 1)
         cpu = {"value": sps, "unit": "steps/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": sample}
     except Exception as e:  # reported, not fatal
         cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("adv_step_fp32_bytes")
-        except Exception:
-            traffic = None
+    zp = passes.get("z", {})
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -297,10 +331,14 @@ def run_ours(args, rank, world, local_rank):
         "speedup_vs_fp64": ms_step64 / ms_step,
         "rel_l2_err_vs_fp64": err,
         "err_after_steps": args.warmup + args.steps,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "one adv step (36 r2r_pass_kernel launches); algorithmic bytes "
-                               "= 4 B x 256^3 x 32 compulsory field transfers"},
+        "roofline": {"bound": "hbm", "achieved": zp.get("gbs"), "peak": peak, "unit": "GB/s",
+                     "frac": zp.get("frac"), "traffic": profile_traffic("r2r_fast_z_pass_256cube_fp32.md"),
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "kernel": "r2r_fast_kernel<float,256,z> plain DCT-II pass (the largest share of the "
+                               "adv step's device time): algorithmic bytes per launch = 2 x 4 B x 256^3 "
+                               "(one field read, one written), average launch time on a 6-field ring"},
+        "step_roofline": {"achieved": achieved_step, "peak": peak, "unit": "GB/s", "frac": achieved_step / peak,
+                          "basis": "4 B x 256^3 x 32 compulsory field transfers per adv step"},
         "pass_kernels": passes,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 8 * N ** 3,
@@ -344,8 +382,8 @@ def run_kernel_only(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "step"], default=None,
                     help="launch one kernel family a few times (for profilers) and exit")
