@@ -332,10 +332,10 @@ def run_ours(args, rank, world, local_rank):
         "rel_l2_err_vs_fp64": err,
         "err_after_steps": args.warmup + args.steps,
         "roofline": {"bound": "hbm", "achieved": zp.get("gbs"), "peak": peak, "unit": "GB/s",
-                     "frac": zp.get("frac"), "traffic": profile_traffic("r2r_fast_z_pass_256cube_fp32.md"),
+                     "frac": zp.get("frac"), "traffic": profile_traffic("r2r_rdz_z_pass_256cube_fp32.md"),
                      "peak_source": f"{peak_kind} hbm_gbs",
-                     "kernel": "r2r_fast_kernel<float,256,z> plain DCT-II pass (the largest share of the "
-                               "adv step's device time): algorithmic bytes per launch = 2 x 4 B x 256^3 "
+                     "kernel": "r2r_rdz_kernel<float,256> plain DCT-II pass along z (the largest share of "
+                               "the adv step's device time): algorithmic bytes per launch = 2 x 4 B x 256^3 "
                                "(one field read, one written), average launch time on a 6-field ring"},
         "step_roofline": {"achieved": achieved_step, "peak": peak, "unit": "GB/s", "frac": achieved_step / peak,
                           "basis": "4 B x 256^3 x 32 compulsory field transfers per adv step"},
@@ -354,6 +354,7 @@ def run_kernel_only(args):
     """A few launches of one kernel family for profiling (ncu): no timing, no JSON.
 
     pass-z | pass-y | pass-x: one plain DCT-II axis pass on a 256^3 field (2 fields held).
+    r2r3d: one plain 3-D DCT-III (the plane kernel for z and y where it applies, then x).
     step: loop bodies of the adv model (all its kernels).
     """
     import torch
@@ -370,6 +371,13 @@ def run_kernel_only(args):
             axis = {"pass-z": 2, "pass-y": 1, "pass-x": 0}[args.kernel_only]
             for _ in range(args.reps):
                 s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, 0)
+        elif args.kernel_only == "r2r3d":
+            dt = torch.float32 if prec == smadft.FP32 else torch.float64
+            x = torch.randn((n, n, n), device="cuda", dtype=dt)
+            y = torch.empty_like(x)
+            torch.cuda.synchronize()
+            for _ in range(args.reps):
+                s.r2r3d_device(x.data_ptr(), y.data_ptr(), (1, 1, 1))
         else:
             p2 = smadft.params(smadft.ADV, (n, n, n), **CFG)
             s.set_psi(smadft.ic_conics(p2, A=1.328, count=4, rmin=3.0, rmax=6.0, seed=1))
@@ -385,7 +393,7 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "step"], default=None,
+    ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "r2r3d", "step"], default=None,
                     help="launch one kernel family a few times (for profilers) and exit")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--shape", type=int, default=N)

@@ -12,7 +12,9 @@
 #include <vector>
 
 #include "r2r_fast.cuh"
+#include "r2r_plane.cuh"
 #include "r2r_rd.cuh"
+#include "r2r_rdz.cuh"
 #include "r2r_pass.cuh"
 #include "smadft.h"
 
@@ -77,6 +79,8 @@ struct Ctx {
     long long launches = 0;     // kernels launched by this context
     bool use_fast = true;       // compile-time-length pass kernels where available
     bool use_rd = true;         // register-direct kernels for plain strided passes
+    bool use_rdz = true;        // register-direct z kernel for plain z passes (SMADFT_RDZ=0: staged)
+    bool use_plane = false;     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
     double *stage = nullptr;    // FP64 staging field for host-psi steps (allocated on first use)
 
     template <typename T>
@@ -207,8 +211,29 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
+// plain z pass of length N through the register-direct z kernel (in == out allowed)
+template <typename T, int N>
+int launch_rdz(Ctx &c, int kind, const T *in, T *out)
+{
+    const PlanDev &pd = c.plans.at(N);
+    const long long rows = (long long)c.g.nx * c.g.ny;
+    const long long tiles = (rows + 2 * kRdLines - 1) / (2 * kRdLines);
+    constexpr size_t smem = rd_smem_bytes<T, N>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    r2r_rdz_kernel<T, N><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+        rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h));
+    SMADFT_CUDA(cudaGetLastError());
+    c.launches++;
+    return SMADFT_OK;
+}
+
 // Line lengths with a compile-time staged kernel (the configs' grids); others use the
-// generic one.  Strided axes of length 64/128/256 run the register-direct kernel instead.
+// generic one.  Lengths 64/128/256 run the register-direct kernels instead: strided axes
+// with any loader and storer, the z axis for plain arrays.
 #define SMADFT_FAST_SIZES(X) X(64) X(96) X(128) X(160) X(256)
 #define SMADFT_FAST_SIZES_STRIDED(X) X(96) X(160)
 
@@ -222,6 +247,15 @@ int launch_axis(Ctx &c, int kind, LD ld, ST st)
             case 64: return launch_rd<T, 64, AXIS>(c, kind, ld, st);
             case 128: return launch_rd<T, 128, AXIS>(c, kind, ld, st);
             case 256: return launch_rd<T, 256, AXIS>(c, kind, ld, st);
+            default: break;
+            }
+        }
+    } else if constexpr (std::is_same<LD, LoadArr<T>>::value && std::is_same<ST, StoreArr<T>>::value) {
+        if (c.use_rd && c.use_rdz) {
+            switch (n) {
+            case 64: return launch_rdz<T, 64>(c, kind, ld.p, st.p);
+            case 128: return launch_rdz<T, 128>(c, kind, ld.p, st.p);
+            case 256: return launch_rdz<T, 256>(c, kind, ld.p, st.p);
             default: break;
             }
         }
@@ -270,18 +304,99 @@ int convert(Ctx &c, const S *src, D *dst)
     return SMADFT_OK;
 }
 
-// 3-D transform: y pass (custom loader) -> z pass -> x pass (custom storer), in place on
-// the scratch field.  The fused loader and storer run in the register-direct strided
-// kernels; the z pass in between only moves the scratch field.
+// z and y passes of NC components per plane in one launch: one cluster of N / 32 CTAs per
+// (plane, component)
+template <typename T, int N, int NC, class LD>
+int launch_plane(Ctx &c, const PlaneKinds<NC> &kinds, LD ld, const StoreMulti<T, NC> &st)
+{
+    const PlanDev &pd = c.plans.at(N);
+    constexpr size_t smem = plane_smem_bytes<T, N>();
+    using ST = StoreMulti<T, NC>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_plane_kernel<T, N, NC, LD, ST>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)c.g.nx * NC * PlaneInfo<N>::C);
+    cfg.blockDim = dim3(RdInfo<N>::THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = PlaneInfo<N>::C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SMADFT_CUDA(cudaLaunchKernelEx(&cfg, r2r_plane_kernel<T, N, NC, LD, ST>, c.g, kinds, ld,
+                                   reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st));
+    c.launches++;
+    return SMADFT_OK;
+}
+
+template <typename T, int NC, class LD>
+int launch_plane_n(Ctx &c, const PlaneKinds<NC> &kinds, LD ld, const StoreMulti<T, NC> &st)
+{
+    switch (c.g.nz) {
+    case 64: return launch_plane<T, 64, NC>(c, kinds, ld, st);
+    case 128: return launch_plane<T, 128, NC>(c, kinds, ld, st);
+    default: return launch_plane<T, 256, NC>(c, kinds, ld, st);
+    }
+}
+
+inline bool plane_ok(const Ctx &c)
+{
+    return c.use_plane && c.g.ny == c.g.nz && (c.g.nz == 64 || c.g.nz == 128 || c.g.nz == 256);
+}
+
+// 3-D transform with the custom loader in the first pass and the custom storer in the last,
+// through the scratch field: for ny = nz in {64, 128, 256} the fused z + y plane kernel then
+// the x pass (two sweeps over HBM), otherwise y pass -> z pass -> x pass, all in place on
+// the scratch field (the z pass in between only moves the scratch field).
 template <typename T, class LD, class ST>
 int r2r3d(Ctx &c, int kx, int ky, int kz, LD ld, ST st)
 {
     T *tmp = c.f<T>(S_TMP);
-    int rc = launch_axis<T, 1>(c, ky, ld, StoreArr<T>{tmp});
+    int rc;
+    if (plane_ok(c)) {
+        rc = launch_plane_n<T, 1>(c, PlaneKinds<1>{{ky}, {kz}}, make_multi(ld), StoreMulti<T, 1>{{tmp}});
+        if (rc) return rc;
+        return launch_axis<T, 0>(c, kx, LoadArr<T>{tmp}, st);
+    }
+    rc = launch_axis<T, 1>(c, ky, ld, StoreArr<T>{tmp});
     if (rc) return rc;
     rc = launch_axis<T, 2>(c, kz, LoadArr<T>{tmp}, StoreArr<T>{tmp});
     if (rc) return rc;
     return launch_axis<T, 0>(c, kx, LoadArr<T>{tmp}, st);
+}
+
+// NC 3-D transforms whose loaders share input fields: component m goes from loader ls[m]
+// to field out[m] with kinds (kx[m], ky[m], kz[m]).  Plane path: one plane launch for all
+// components (their shared reads meet in L2), then the x pass of each in place; otherwise
+// NC separate transforms through the scratch field.
+template <typename T, int NC, class... L>
+int r2r3d_multi(Ctx &c, const int (&kx)[NC], const int (&ky)[NC], const int (&kz)[NC], T *const (&out)[NC], L... ls)
+{
+    static_assert(sizeof...(L) == NC, "one loader per component");
+    int rc = SMADFT_OK;
+    if (plane_ok(c)) {
+        PlaneKinds<NC> pk;
+        StoreMulti<T, NC> sm;
+        for (int m = 0; m < NC; m++) {
+            pk.ky[m] = ky[m];
+            pk.kz[m] = kz[m];
+            sm.p[m] = out[m];
+        }
+        if ((rc = launch_plane_n<T, NC>(c, pk, make_multi(ls...), sm))) return rc;
+        for (int m = 0; m < NC; m++)
+            if ((rc = launch_axis<T, 0>(c, kx[m], LoadArr<T>{out[m]}, StoreArr<T>{out[m]}))) return rc;
+        return rc;
+    }
+    int m = 0;
+    ((rc = rc ? rc : r2r3d<T>(c, kx[m], ky[m], kz[m], ls, StoreArr<T>{out[m]}), m++), ...);
+    return rc;
 }
 
 }  // namespace smadft

@@ -20,6 +20,15 @@ __device__ __forceinline__ T nl3(T p, T beta, T gamma)   // beta psi^3 - gamma p
     return beta * p3 - gamma * (p3 * p2);
 }
 
+// 1 / x for x > 0.  FP32: __fdividef (hardware reciprocal, at most 2 ulp), far inside the
+// FP32 path's error budget; FP64: the correctly rounded reciprocal the FP64 parity needs.
+template <typename T>
+__device__ __forceinline__ T recip(T x)
+{
+    if constexpr (sizeof(T) == 4) return __fdividef(1.0f, x);
+    else return T(1) / x;
+}
+
 // ---------------------------------------------------------------- loaders -------------
 // All functors follow the vector interface of r2r_pass.cuh: V consecutive elements along z
 // (idx .. idx+V-1 at (i, j, k .. k+V-1)); same-index fields use 16-byte loads, index-shifted
@@ -135,7 +144,7 @@ struct LdStokes {
                 const bool kz = kk != 0;
                 const T szr = Sz[kz ? qn - 1 + u : qn + u];       // (i+1, j, k-1)
                 const T syv = jy ? sy[u] : T(0), sz = kz ? szr : T(0);
-                const T inv = T(1) / (a2 + qk * qk);
+                const T inv = recip<T>(a2 + qk * qk);
                 const T dot = si * sx[u] + qj * syv + qk * sz;
                 T v = snu * inv * (sx[u] - si * inv * dot);
                 if (DIVV) v = v + snu * inv * (s.nu * si * d[u]);
@@ -158,7 +167,7 @@ struct LdStokes {
                 const bool kz = kk != 0;
                 const T szr = Sz[kz ? qj1 - 1 + u : qj1 + u];     // (i, j+1, k-1)
                 const T sxv = ix ? sx[u] : T(0), sz = kz ? szr : T(0);
-                const T inv = T(1) / (a2 + qk * qk);
+                const T inv = recip<T>(a2 + qk * qk);
                 const T dot = qi * sxv + sj * syv[u] + qk * sz;
                 T v = snu * inv * (syv[u] - sj * inv * dot);
                 if (DIVV) v = v + snu * inv * (s.nu * sj * d[u]);
@@ -180,7 +189,7 @@ struct LdStokes {
                 const T sxr = Sx[ix ? qk1 - s.nyz : qk1];         // (i-1, j, k+1)
                 const T syr = Sy[jy ? qk1 - s.nz : qk1];          // (i, j-1, k+1)
                 const T sx = ix ? sxr : T(0), sy = jy ? syr : T(0);
-                const T inv = T(1) / (a2 + sk * sk);
+                const T inv = recip<T>(a2 + sk * sk);
                 const T dot = qi * sx + qj * sy + sk * szv[u];
                 T v = snu * inv * (szv[u] - sk * inv * dot);
                 if (DIVV) v = v + snu * inv * (s.nu * sk * dv[qk1]);

@@ -17,6 +17,8 @@
 // warp shuffle per value: butterflies j and R1 - j sit in the two halves of one warp.
 #pragma once
 
+#include <type_traits>
+
 #include "r2r_fast.cuh"
 
 namespace smadft {
@@ -43,12 +45,252 @@ struct RdInfo {
 template <typename T, int N>
 constexpr size_t rd_smem_bytes() { return ((size_t)kRdLines * RdInfo<N>::LD + 2 * N) * sizeof(cpx<T>); }
 
+// CTAs per SM the register budget is sized for: FP32 passes over a plain array fit three
+// (80 registers), the fused multi-field loaders and FP64 keep two
+template <typename T, class LD>
+constexpr int rd_min_blocks() { return (sizeof(T) == 4 && std::is_same<LD, LoadArr<T>>::value) ? 3 : 2; }
+
 // natural sample index whose Makhoul position is p (inverse of makhoul_pos)
 template <int N>
 __device__ __forceinline__ int makhoul_src(int p) { return p < N / 2 ? 2 * p : 2 * (N - 1 - p) + 1; }
 
+// The transform of one packed complex line by thread (line c, butterfly j) of warp wi: v
+// holds the R0 stage-0 points j + q R1 (Makhoul-permuted for the forward kinds, DST-II
+// signs applied; natural or reversed order for the inverse kinds); x1 receives the
+// output points, whose line positions rd_out_pos gives.  `line` is this thread's complex
+// line in the CTA's exchange buffer.  Contains __syncthreads(): every thread of the CTA
+// calls it.
+//
+// ZMAP selects the lane layout of r2r_rdz_kernel (lane = butterfly j of one line, see
+// r2r_rdz.cuh): the pairings then go to butterfly R1 - j by an indexed shuffle, and
+// butterfly 0, which pairs with itself, takes its own path after the shuffled one.
+template <typename T, int N, bool ZMAP = false>
+__device__ __forceinline__ void rd_fft(cpx<T> (&v)[RdInfo<N>::R0],
+                                       cpx<T> (&x1)[RdInfo<N>::R0 / RdInfo<N>::R1 > 0 ? RdInfo<N>::R0 / RdInfo<N>::R1 : 1]
+                                                   [RdInfo<N>::R1],
+                                       cpx<T> *line, const cpx<T> *wt, const cpx<T> *ht, int j, int wi, bool fwd,
+                                       bool sine)
+{
+    using RI = RdInfo<N>;
+    constexpr int R0 = RI::R0, R1 = RI::R1;
+    constexpr int BPT = R0 / R1 > 0 ? R0 / R1 : 1;
+    if (!fwd) {
+        // DCT-III pre-twiddle Z_p = V_A[p] + i V_B[p], V[p] = exp(+i pi p/2N)(X_p - i X_{N-p}),
+        // X_N = 0; DST-III reads the line reversed.  X_{N-p} comes from the partner lane (or
+        // the thread itself in warp 0); each pair of points is rewritten in place together so
+        // only one array stays live.
+        auto ztw = [&](int q, cpx<T> xa, cpx<T> xb) -> cpx<T> {
+            const cpx<T> hh = ht[j + q * R1];
+            const T cc = hh.x, ss = hh.y;
+            const T var = cc * xa.x + ss * xb.x, vai = ss * xa.x - cc * xb.x;
+            const T vbr = cc * xa.y + ss * xb.y, vbi = ss * xa.y - cc * xb.y;
+            return {var - vbi, vai + vbr};
+        };
+        if constexpr (ZMAP) {
+            // butterfly j >= 1: partner point of q is R0 - 1 - q in butterfly R1 - j (lane pl;
+            // j = R1/2 reads itself); butterfly 0 keeps its values for the path below
+            const int lane = threadIdx.x & 31;
+            const int pl = j == 0 ? lane : lane + R1 - 2 * j;
+#pragma unroll
+            for (int q = 0; q < R0 / 2; q++) {
+                const int qb = R0 - 1 - q;
+                cpx<T> pa, pb;
+                pa.x = __shfl_sync(0xffffffffu, v[qb].x, pl);
+                pa.y = __shfl_sync(0xffffffffu, v[qb].y, pl);
+                pb.x = __shfl_sync(0xffffffffu, v[q].x, pl);
+                pb.y = __shfl_sync(0xffffffffu, v[q].y, pl);
+                const cpx<T> za = ztw(q, v[q], pa), zb = ztw(qb, v[qb], pb);
+                if (j != 0) {
+                    v[q] = za;
+                    v[qb] = zb;
+                }
+            }
+            if (j == 0) {
+                v[0] = ztw(0, v[0], cpx<T>{T(0), T(0)});
+                v[R0 / 2] = ztw(R0 / 2, v[R0 / 2], v[R0 / 2]);
+#pragma unroll
+                for (int q = 1; q < R0 / 2; q++) {
+                    const int qb = R0 - q;
+                    const cpx<T> za = ztw(q, v[q], v[qb]), zb = ztw(qb, v[qb], v[q]);
+                    v[q] = za;
+                    v[qb] = zb;
+                }
+            }
+        } else if (wi != 0 || j == R1 / 2) {
+            // partner point of q is R0 - 1 - q (in lane ^ 16, or here for j = R1/2)
+#pragma unroll
+            for (int q = 0; q < R0 / 2; q++) {
+                const int qb = R0 - 1 - q;
+                cpx<T> pa, pb;
+                if (wi != 0) {
+                    pa.x = __shfl_xor_sync(0xffffffffu, v[qb].x, 16);
+                    pa.y = __shfl_xor_sync(0xffffffffu, v[qb].y, 16);
+                    pb.x = __shfl_xor_sync(0xffffffffu, v[q].x, 16);
+                    pb.y = __shfl_xor_sync(0xffffffffu, v[q].y, 16);
+                } else {
+                    pa = v[qb];
+                    pb = v[q];
+                }
+                const cpx<T> za = ztw(q, v[q], pa), zb = ztw(qb, v[qb], pb);
+                v[q] = za;
+                v[qb] = zb;
+            }
+        } else {
+            // j = 0: partner of q is R0 - q (q = 0 pairs with X_N = 0, q = R0/2 with itself)
+            v[0] = ztw(0, v[0], cpx<T>{T(0), T(0)});
+            v[R0 / 2] = ztw(R0 / 2, v[R0 / 2], v[R0 / 2]);
+#pragma unroll
+            for (int q = 1; q < R0 / 2; q++) {
+                const int qb = R0 - q;
+                const cpx<T> za = ztw(q, v[q], v[qb]), zb = ztw(qb, v[qb], v[q]);
+                v[q] = za;
+                v[qb] = zb;
+            }
+        }
+    }
+
+    // ---- stage 0: radix R0 over stride R1, twiddles W_N^(j q), into shared memory
+    if (fwd) codelet<R0, T, false>(v);
+    else codelet<R0, T, true>(v);
+#pragma unroll
+    for (int q = 0; q < R0; q++) {
+        cpx<T> o = v[q];
+        if (q > 0) o = fwd ? cmul(o, tw<T, false>(wt, j * q)) : cmul(o, tw<T, true>(wt, j * q));
+        line[RI::phys(j + q * R1)] = o;
+    }
+    __syncthreads();
+
+    // ---- stage 1: radix R1 over contiguous blocks; block b holds X[b + R0 q] afterwards
+#pragma unroll
+    for (int r = 0; r < BPT; r++) {
+        const int b = j + r * R1;
+        cpx<T> *pb = line + RI::phys(b * R1);
+#pragma unroll
+        for (int q = 0; q < R1; q++) x1[r][q] = pb[q];
+        if (fwd) codelet<R1, T, false>(x1[r]);
+        else codelet<R1, T, true>(x1[r]);
+    }
+
+    // ---- outputs: (real line A, real line B) pairs in x1
+    if (!fwd) {
+        // DCT-III output y[2m] = v[m], y[2m+1] = v[N-1-m]; DST-III negates odd outputs
+#pragma unroll
+        for (int r = 0; r < BPT; r++)
+#pragma unroll
+            for (int q = 0; q < R1; q++) {
+                const int m = j + r * R1 + R0 * q;
+                const int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
+                if (sine && (o & 1)) x1[r][q] = {-x1[r][q].x, -x1[r][q].y};
+            }
+    } else {
+        // DCT-II post-twiddle pairs X[k] with X[N-k]
+        if constexpr (BPT == 1) {
+            // X[N - k] is block R1 - j at q' = R1 - 1 - q (lane ^ 16, or this thread for
+            // j = R1/2), or block 0 at q' = (R1 - q) mod R1 for j = 0; each pair (q, q') is
+            // rewritten in place together
+            auto post = [&](int q, cpx<T> zm) -> cpx<T> {
+                const int kk = j + R0 * q;
+                const cpx<T> hh = ht[kk];
+                return {dct2_out(x1[0][q], zm, hh, 0), dct2_out(x1[0][q], zm, hh, 1)};
+            };
+            if constexpr (ZMAP) {
+                const int lane = threadIdx.x & 31;
+                const int pl = j == 0 ? lane : lane + R1 - 2 * j;
+#pragma unroll
+                for (int q = 0; q < R1 / 2; q++) {
+                    const int qb = R1 - 1 - q;
+                    cpx<T> pa, pb;
+                    pa.x = __shfl_sync(0xffffffffu, x1[0][qb].x, pl);
+                    pa.y = __shfl_sync(0xffffffffu, x1[0][qb].y, pl);
+                    pb.x = __shfl_sync(0xffffffffu, x1[0][q].x, pl);
+                    pb.y = __shfl_sync(0xffffffffu, x1[0][q].y, pl);
+                    const cpx<T> oa = post(q, pa), ob = post(qb, pb);
+                    if (j != 0) {
+                        x1[0][q] = oa;
+                        x1[0][qb] = ob;
+                    }
+                }
+                if (j == 0) {
+                    const cpx<T> o0 = post(0, x1[0][0]);
+                    const cpx<T> oh = post(R1 / 2, x1[0][R1 / 2]);
+#pragma unroll
+                    for (int q = 1; q < R1 / 2; q++) {
+                        const int qb = R1 - q;
+                        const cpx<T> oa = post(q, x1[0][qb]), ob = post(qb, x1[0][q]);
+                        x1[0][q] = oa;
+                        x1[0][qb] = ob;
+                    }
+                    x1[0][0] = o0;
+                    x1[0][R1 / 2] = oh;
+                }
+            } else if (wi != 0 || j == R1 / 2) {
+#pragma unroll
+                for (int q = 0; q < R1 / 2; q++) {
+                    const int qb = R1 - 1 - q;
+                    cpx<T> pa, pb;
+                    if (wi != 0) {
+                        pa.x = __shfl_xor_sync(0xffffffffu, x1[0][qb].x, 16);
+                        pa.y = __shfl_xor_sync(0xffffffffu, x1[0][qb].y, 16);
+                        pb.x = __shfl_xor_sync(0xffffffffu, x1[0][q].x, 16);
+                        pb.y = __shfl_xor_sync(0xffffffffu, x1[0][q].y, 16);
+                    } else {
+                        pa = x1[0][qb];
+                        pb = x1[0][q];
+                    }
+                    const cpx<T> oa = post(q, pa), ob = post(qb, pb);
+                    x1[0][q] = oa;
+                    x1[0][qb] = ob;
+                }
+            } else {
+                const cpx<T> o0 = post(0, x1[0][0]);
+                const cpx<T> oh = post(R1 / 2, x1[0][R1 / 2]);
+#pragma unroll
+                for (int q = 1; q < R1 / 2; q++) {
+                    const int qb = R1 - q;
+                    const cpx<T> oa = post(q, x1[0][qb]), ob = post(qb, x1[0][q]);
+                    x1[0][q] = oa;
+                    x1[0][qb] = ob;
+                }
+                x1[0][0] = o0;
+                x1[0][R1 / 2] = oh;
+            }
+        } else {
+            // through shared memory (each thread rewrites only its own blocks first)
+#pragma unroll
+            for (int r = 0; r < BPT; r++) {
+                cpx<T> *pb = line + RI::phys((j + r * R1) * R1);
+#pragma unroll
+                for (int q = 0; q < R1; q++) pb[q] = x1[r][q];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < BPT; r++)
+#pragma unroll
+                for (int q = 0; q < R1; q++) {
+                    const int kk = j + r * R1 + R0 * q;
+                    const int km = kk == 0 ? 0 : N - kk;
+                    const cpx<T> zm = line[RI::phys((km % R0) * R1 + km / R0)];
+                    const cpx<T> hh = ht[kk];
+                    const cpx<T> zk = x1[r][q];
+                    x1[r][q] = {dct2_out(zk, zm, hh, 0), dct2_out(zk, zm, hh, 1)};
+                }
+        }
+    }
+
+}
+
+// line position of output point pnt of butterfly j (see rd_fft)
+template <int N>
+__device__ __forceinline__ int rd_out_pos(int j, int pnt, bool fwd, bool sine)
+{
+    constexpr int R0 = RdInfo<N>::R0, R1 = RdInfo<N>::R1;
+    const int kk = j + (pnt / R1) * R1 + R0 * (pnt % R1);   // X index held by point pnt
+    if (fwd) return sine ? N - 1 - kk : kk;
+    return kk < N / 2 ? 2 * kk : 2 * (N - 1 - kk) + 1;
+}
+
 template <typename T, int N, int AXIS, class LD, class ST>
-__global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, int kind, int tiles_b, LD ld,
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2r_rd_kernel(Geom g, int kind, int tiles_b, LD ld,
                                                                        const cpx<T> *__restrict__ wt_g,
                                                                        const cpx<T> *__restrict__ ht_g, ST st)
 {
@@ -114,155 +356,10 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_rd_kernel(Geom g, i
             for (int q = 0; q < R0; q++)
                 if (src_pos(q) & 1) v[q] = {-v[q].x, -v[q].y};
         }
-    } else {
-        // DCT-III pre-twiddle Z_p = V_A[p] + i V_B[p], V[p] = exp(+i pi p/2N)(X_p - i X_{N-p}),
-        // X_N = 0; DST-III reads the line reversed.  X_{N-p} comes from the partner lane (or
-        // the thread itself in warp 0); each pair of points is rewritten in place together so
-        // only one array stays live.
-        auto ztw = [&](int q, cpx<T> xa, cpx<T> xb) -> cpx<T> {
-            const cpx<T> hh = ht[j + q * R1];
-            const T cc = hh.x, ss = hh.y;
-            const T var = cc * xa.x + ss * xb.x, vai = ss * xa.x - cc * xb.x;
-            const T vbr = cc * xa.y + ss * xb.y, vbi = ss * xa.y - cc * xb.y;
-            return {var - vbi, vai + vbr};
-        };
-        if (wi != 0 || j == R1 / 2) {
-            // partner point of q is R0 - 1 - q (in lane ^ 16, or here for j = R1/2)
-#pragma unroll
-            for (int q = 0; q < R0 / 2; q++) {
-                const int qb = R0 - 1 - q;
-                cpx<T> pa, pb;
-                if (wi != 0) {
-                    pa.x = __shfl_xor_sync(0xffffffffu, v[qb].x, 16);
-                    pa.y = __shfl_xor_sync(0xffffffffu, v[qb].y, 16);
-                    pb.x = __shfl_xor_sync(0xffffffffu, v[q].x, 16);
-                    pb.y = __shfl_xor_sync(0xffffffffu, v[q].y, 16);
-                } else {
-                    pa = v[qb];
-                    pb = v[q];
-                }
-                const cpx<T> za = ztw(q, v[q], pa), zb = ztw(qb, v[qb], pb);
-                v[q] = za;
-                v[qb] = zb;
-            }
-        } else {
-            // j = 0: partner of q is R0 - q (q = 0 pairs with X_N = 0, q = R0/2 with itself)
-            v[0] = ztw(0, v[0], cpx<T>{T(0), T(0)});
-            v[R0 / 2] = ztw(R0 / 2, v[R0 / 2], v[R0 / 2]);
-#pragma unroll
-            for (int q = 1; q < R0 / 2; q++) {
-                const int qb = R0 - q;
-                const cpx<T> za = ztw(q, v[q], v[qb]), zb = ztw(qb, v[qb], v[q]);
-                v[q] = za;
-                v[qb] = zb;
-            }
-        }
     }
-
-    // ---- stage 0: radix R0 over stride R1, twiddles W_N^(j q), into shared memory
-    cpx<T> *line = buf + c * RI::LD;
-    if (fwd) codelet<R0, T, false>(v);
-    else codelet<R0, T, true>(v);
-#pragma unroll
-    for (int q = 0; q < R0; q++) {
-        cpx<T> o = v[q];
-        if (q > 0) o = fwd ? cmul(o, tw<T, false>(wt, j * q)) : cmul(o, tw<T, true>(wt, j * q));
-        line[RI::phys(j + q * R1)] = o;
-    }
-    __syncthreads();
-
-    // ---- stage 1: radix R1 over contiguous blocks; block b holds X[b + R0 q] afterwards
     cpx<T> x1[BPT][R1];
-#pragma unroll
-    for (int r = 0; r < BPT; r++) {
-        const int b = j + r * R1;
-        cpx<T> *pb = line + RI::phys(b * R1);
-#pragma unroll
-        for (int q = 0; q < R1; q++) x1[r][q] = pb[q];
-        if (fwd) codelet<R1, T, false>(x1[r]);
-        else codelet<R1, T, true>(x1[r]);
-    }
-
-    // ---- outputs: (real line A, real line B) pairs in x1; line position of point pnt
-    auto out_row = [&](int pnt) -> int {
-        const int kk = j + (pnt / R1) * R1 + R0 * (pnt % R1);   // X index held by point pnt
-        if (fwd) return sine ? N - 1 - kk : kk;
-        return kk < N / 2 ? 2 * kk : 2 * (N - 1 - kk) + 1;
-    };
-    if (!fwd) {
-        // DCT-III output y[2m] = v[m], y[2m+1] = v[N-1-m]; DST-III negates odd outputs
-#pragma unroll
-        for (int r = 0; r < BPT; r++)
-#pragma unroll
-            for (int q = 0; q < R1; q++) {
-                const int m = j + r * R1 + R0 * q;
-                const int o = m < N / 2 ? 2 * m : 2 * (N - 1 - m) + 1;
-                if (sine && (o & 1)) x1[r][q] = {-x1[r][q].x, -x1[r][q].y};
-            }
-    } else {
-        // DCT-II post-twiddle pairs X[k] with X[N-k]
-        if constexpr (BPT == 1) {
-            // X[N - k] is block R1 - j at q' = R1 - 1 - q (lane ^ 16, or this thread for
-            // j = R1/2), or block 0 at q' = (R1 - q) mod R1 for j = 0; each pair (q, q') is
-            // rewritten in place together
-            auto post = [&](int q, cpx<T> zm) -> cpx<T> {
-                const int kk = j + R0 * q;
-                const cpx<T> hh = ht[kk];
-                return {dct2_out(x1[0][q], zm, hh, 0), dct2_out(x1[0][q], zm, hh, 1)};
-            };
-            if (wi != 0 || j == R1 / 2) {
-#pragma unroll
-                for (int q = 0; q < R1 / 2; q++) {
-                    const int qb = R1 - 1 - q;
-                    cpx<T> pa, pb;
-                    if (wi != 0) {
-                        pa.x = __shfl_xor_sync(0xffffffffu, x1[0][qb].x, 16);
-                        pa.y = __shfl_xor_sync(0xffffffffu, x1[0][qb].y, 16);
-                        pb.x = __shfl_xor_sync(0xffffffffu, x1[0][q].x, 16);
-                        pb.y = __shfl_xor_sync(0xffffffffu, x1[0][q].y, 16);
-                    } else {
-                        pa = x1[0][qb];
-                        pb = x1[0][q];
-                    }
-                    const cpx<T> oa = post(q, pa), ob = post(qb, pb);
-                    x1[0][q] = oa;
-                    x1[0][qb] = ob;
-                }
-            } else {
-                const cpx<T> o0 = post(0, x1[0][0]);
-                const cpx<T> oh = post(R1 / 2, x1[0][R1 / 2]);
-#pragma unroll
-                for (int q = 1; q < R1 / 2; q++) {
-                    const int qb = R1 - q;
-                    const cpx<T> oa = post(q, x1[0][qb]), ob = post(qb, x1[0][q]);
-                    x1[0][q] = oa;
-                    x1[0][qb] = ob;
-                }
-                x1[0][0] = o0;
-                x1[0][R1 / 2] = oh;
-            }
-        } else {
-            // through shared memory (each thread rewrites only its own blocks first)
-#pragma unroll
-            for (int r = 0; r < BPT; r++) {
-                cpx<T> *pb = line + RI::phys((j + r * R1) * R1);
-#pragma unroll
-                for (int q = 0; q < R1; q++) pb[q] = x1[r][q];
-            }
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < BPT; r++)
-#pragma unroll
-                for (int q = 0; q < R1; q++) {
-                    const int kk = j + r * R1 + R0 * q;
-                    const int km = kk == 0 ? 0 : N - kk;
-                    const cpx<T> zm = line[RI::phys((km % R0) * R1 + km / R0)];
-                    const cpx<T> hh = ht[kk];
-                    const cpx<T> zk = x1[r][q];
-                    x1[r][q] = {dct2_out(zk, zm, hh, 0), dct2_out(zk, zm, hh, 1)};
-                }
-        }
-    }
+    rd_fft<T, N>(v, x1, buf + c * RI::LD, wt, ht, j, wi, fwd, sine);
+    auto out_row = [&](int pnt) -> int { return rd_out_pos<N>(j, pnt, fwd, sine); };
 
     // ---- stores: the storer's reads (pre) for a chunk of points go out before its writes
     constexpr int CH = 4;

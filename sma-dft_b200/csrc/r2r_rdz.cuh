@@ -1,0 +1,74 @@
+// r2r_rdz.cuh -- register-direct axis pass along z (the contiguous axis) for the
+// two-stage plans of r2r_rd.cuh (N = R0 x R1: 64 = 8x8, 128 = 16x8, 256 = 16x16).
+//
+// The strided kernel puts 16 lines on the lanes of a half-warp so that one access covers
+// 128 contiguous bytes.  Along z a line is itself contiguous, so here the R1 lanes of a
+// line group are the first-stage butterflies j of one packed complex line (real rows
+// r and r + 1 as real and imaginary parts).  Butterfly j reads the positions of its
+// points j + R1 q straight from global memory into registers: consecutive lanes read
+// consecutive positions (inverse kinds) or every second one (the Makhoul order of the
+// forward kinds, whose other half the same warp reads in another instruction), so each
+// 32-byte sector a warp touches is used in full and the tile is never staged in shared
+// memory.  Shared memory carries only the exchange between the two radix stages; the
+// X[p] / X[N - p] pairings are lane shuffles inside the line group (rd_fft, ZMAP).
+// Outputs go from registers to global memory.  Loads finish before the first barrier and
+// every row belongs to one CTA, so the pass may run in place (in == out).
+#pragma once
+
+#include "r2r_rd.cuh"
+
+namespace smadft {
+
+// rows = number of z lines (nx * ny); a CTA transforms 2 * kRdLines consecutive rows
+template <typename T, int N>
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(long long rows, int kind, const T *in, T *out,
+                                                                        const cpx<T> *__restrict__ wt_g,
+                                                                        const cpx<T> *__restrict__ ht_g)
+{
+    using RI = RdInfo<N>;
+    constexpr int R0 = RI::R0, R1 = RI::R1, NT = RI::THREADS;
+    constexpr int BPT = R0 / R1 > 0 ? R0 / R1 : 1;
+    constexpr int NP = BPT * R1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T> *buf = reinterpret_cast<cpx<T> *>(smem_raw);
+    cpx<T> *wt = buf + kRdLines * RI::LD;
+    cpx<T> *ht = wt + N;
+    for (int m = threadIdx.x; m < N; m += NT) {
+        wt[m] = wt_g[m];
+        ht[m] = ht_g[m];
+    }
+    const int j = threadIdx.x % R1;                 // first-stage butterfly (lane in its group)
+    const int c = threadIdx.x / R1;                 // complex line of the CTA
+    const long long ra = (long long)blockIdx.x * (2 * kRdLines) + 2 * c;   // real rows ra, ra + 1
+    const bool oka = ra < rows, okb = ra + 1 < rows;
+    const long long ia = (oka ? ra : 0) * N, ib = (okb ? ra + 1 : 0) * N;
+    const bool fwd = (kind == K_DCT2 || kind == K_DST2);
+    const bool sine = (kind == K_DST2 || kind == K_DST3);
+
+    cpx<T> v[R0];
+#pragma unroll
+    for (int q = 0; q < R0; q++) {
+        const int p = j + q * R1;
+        const int n = fwd ? makhoul_src<N>(p) : (sine ? N - 1 - p : p);
+        T a = in[ia + n], b = in[ib + n];
+        if (!oka) a = T(0);
+        if (!okb) b = T(0);
+        if (fwd && sine && (n & 1)) {                // DST-II negates odd natural samples
+            a = -a;
+            b = -b;
+        }
+        v[q] = {a, b};
+    }
+    __syncthreads();                                 // twiddle tables
+    cpx<T> x1[BPT][R1];
+    rd_fft<T, N, true>(v, x1, buf + c * RI::LD, wt, ht, j, threadIdx.x >> 5, fwd, sine);
+#pragma unroll
+    for (int pnt = 0; pnt < NP; pnt++) {
+        const cpx<T> z = x1[pnt / R1][pnt % R1];
+        const int o = rd_out_pos<N>(j, pnt, fwd, sine);
+        if (oka) out[ia + o] = z.x;
+        if (okb) out[ib + o] = z.y;
+    }
+}
+
+}  // namespace smadft

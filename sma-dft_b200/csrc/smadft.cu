@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -345,6 +346,10 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     c.Lz = p->nz * 2.0 * M_PI / (p->q0 * p->nw);
     c.dx = c.Lx / p->nx; c.dy = c.Ly / p->ny; c.dz = c.Lz / p->nz;
     c.scale = 0.125 / ((double)p->nx * p->ny * p->nz);
+    // SMADFT_PLANE=1 selects the fused z + y plane kernel (r2r_plane.cuh) where ny = nz allows;
+    // the separate axis passes are the default (faster in FP32 on B200)
+    if (const char *e = std::getenv("SMADFT_PLANE")) c.use_plane = e[0] != '0';
+    if (const char *e = std::getenv("SMADFT_RDZ")) c.use_rdz = e[0] != '0';
     auto bail = [&](int code) { smadft_destroy(h); return code; };
     if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);

@@ -13,27 +13,50 @@ int adv_step(Ctx &c)
     T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
     T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
     int rc;
-    // psi and grad psi from psihat (adv/cosAdvTrackMult.cpp:904-975)
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{psi}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdGrad<T, 0>{s, ph}, StoreArr<T>{gx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdGrad<T, 1>{s, ph}, StoreArr<T>{gy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdGrad<T, 2>{s, ph}, StoreArr<T>{gz}))) return rc;
-    // Sp2 = iCT(-L psihat) (:980-991)
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdNegLin<T>{s, ph}, StoreArr<T>{sp2}))) return rc;
+    // psi, grad psi and Sp2 = iCT(-L psihat), all from psihat (adv/cosAdvTrackMult.cpp:904-991)
+    {
+        const int kx[5] = {K_DCT3, K_DST3, K_DCT3, K_DCT3, K_DCT3};
+        const int ky[5] = {K_DCT3, K_DCT3, K_DST3, K_DCT3, K_DCT3};
+        const int kz[5] = {K_DCT3, K_DCT3, K_DCT3, K_DST3, K_DCT3};
+        T *const out[5] = {psi, gx, gy, gz, sp2};
+        if ((rc = r2r3d_multi<T, 5>(c, kx, ky, kz, out, LoadArr<T>{ph}, LdGrad<T, 0>{s, ph}, LdGrad<T, 1>{s, ph},
+                                    LdGrad<T, 2>{s, ph}, LdNegLin<T>{s, ph})))
+            return rc;
+    }
     // force spectra S_c = ST_c(mu d_c psi) (:996-1027)
-    if ((rc = r2r3d<T>(c, K_DST2, K_DCT2, K_DCT2, LdForce<T>{psi, sp2, gx, s.beta, s.gamma}, StoreArr<T>{Sx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DST2, K_DCT2, LdForce<T>{psi, sp2, gy, s.beta, s.gamma}, StoreArr<T>{Sy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DST2, LdForce<T>{psi, sp2, gz, s.beta, s.gamma}, StoreArr<T>{Sz}))) return rc;
+    {
+        const int kx[3] = {K_DST2, K_DCT2, K_DCT2};
+        const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
+        const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
+        T *const out[3] = {Sx, Sy, Sz};
+        if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdForce<T>{psi, sp2, gx, s.beta, s.gamma},
+                                    LdForce<T>{psi, sp2, gy, s.beta, s.gamma},
+                                    LdForce<T>{psi, sp2, gz, s.beta, s.gamma})))
+            return rc;
+    }
     // Stokes velocity (:1030-1286)
-    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr}, StoreArr<T>{vz}))) return rc;
+    {
+        const int kx[3] = {K_DST3, K_DCT3, K_DCT3};
+        const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
+        const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
+        T *const out[3] = {vx, vy, vz};
+        if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr},
+                                    LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr},
+                                    LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr})))
+            return rc;
+    }
     // N = beta psi^3 - gamma psi^5 - v.grad psi, CN/AB2 update (:1290-1365)
     return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
                     LdAdvN<T>{psi, vx, vy, vz, gx, gy, gz, s.beta, s.gamma}, StUpdCN<T>{s, ph, np});
 }
 
+// each precision builds as its own object (SMADFT_INST_FLOAT / SMADFT_INST_DOUBLE); a plain
+// compile without either instantiates both
+#if !defined(SMADFT_INST_DOUBLE)
 template int adv_step<float>(Ctx &);
+#endif
+#if !defined(SMADFT_INST_FLOAT)
 template int adv_step<double>(Ctx &);
+#endif
 
 }  // namespace smadft

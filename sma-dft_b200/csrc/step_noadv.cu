@@ -73,8 +73,14 @@ int plain_pass(Ctx &c, const T *in, T *out, int axis, int kind)
     template int psihat_from_psi<T>(Ctx &);                                \
     template int plain_r2r3d<T>(Ctx &, const T *, T *, int, int, int);     \
     template int plain_pass<T>(Ctx &, const T *, T *, int, int);
+// each precision builds as its own object (SMADFT_INST_FLOAT / SMADFT_INST_DOUBLE); a plain
+// compile without either instantiates both
+#if !defined(SMADFT_INST_DOUBLE)
 SMADFT_INST(float)
+#endif
+#if !defined(SMADFT_INST_FLOAT)
 SMADFT_INST(double)
+#endif
 #undef SMADFT_INST
 
 }  // namespace smadft

@@ -127,6 +127,30 @@ def test_fp64_matches_oracle_fields(model, shape, steps, kw):
                 assert rel_max(s.get(f), o.get(of)) <= tol, f
 
 
+@pytest.mark.parametrize("model,shape,steps,kw", [
+    (smadft.NOADV, (16, 64, 64), 20, dict(dt=0.05)),
+    (smadft.ADV, (12, 64, 64), 10, dict(dt=0.02)),
+    (smadft.QUASI, (8, 64, 64), 8, dict(dt=0.002, kp=0.3755, divv_switch=4)),
+])
+def test_plane_path_matches_oracle(model, shape, steps, kw, monkeypatch):
+    """The opt-in fused z + y plane kernel (SMADFT_PLANE=1, ny = nz = 64) through whole steps."""
+    monkeypatch.setenv("SMADFT_PLANE", "1")
+    p = smadft.params(model, shape, **kw)
+    psi0 = smadft.ic_conics(p, A=1.3, count=2, rmin=1.0, rmax=2.0, noise=1e-3, seed=5)
+    okw = dict(nw=p.nw, dt=p.dt, eps=p.eps, nu=p.nu, kp=p.kp, rho0=p.rho0, divv_switch=p.divv_switch)
+    o = oracle.Oracle(OMODEL[model], shape, **okw)
+    o.set_psi(psi0)
+    o.step(steps)
+    with smadft.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(steps)
+        assert rel_max(s.get("psi"), o.get(oracle.F_PSI)) <= 1e-10
+        if model != smadft.NOADV:
+            tol = 1e-8 if model == smadft.QUASI else 1e-9
+            for f, of in [("vx", oracle.F_VX), ("vz", oracle.F_VZ)]:
+                assert rel_max(s.get(f), o.get(of)) <= tol, f
+
+
 @pytest.mark.parametrize("model,steps,tol", [(smadft.NOADV, 200, 1e-5), (smadft.ADV, 100, 1e-5)])
 def test_fp32_error_vs_fp64(model, steps, tol):
     shape = (48, 40, 64)
