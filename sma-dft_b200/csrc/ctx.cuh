@@ -80,7 +80,12 @@ struct Ctx {
     bool use_fast = true;       // compile-time-length pass kernels where available
     bool use_rd = true;         // register-direct kernels for plain strided passes
     bool use_rdz = true;        // register-direct z kernel for plain z passes (SMADFT_RDZ=0: staged)
-    bool use_plane = false;     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
+    bool use_multi = true;      // one y-pass launch for the components of r2r3d_multi (SMADFT_MULTI=0: off)
+    bool use_fork = true;       // independent per-component passes on forked streams (SMADFT_FORK=0: off)
+    bool use_plane = false;
+    static constexpr int kMaxFork = 5;
+    cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
+    cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
     double *stage = nullptr;    // FP64 staging field for host-psi steps (allocated on first use)
 
     template <typename T>
@@ -159,21 +164,21 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
-template <typename T, int N, int AXIS, class LD, class ST>
-int launch_rd(Ctx &c, int kind, LD ld, ST st)
+template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
+int launch_rd(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
 {
     const PlanDev &pd = c.plans.at(N);
     const int tiles_b = (c.g.nz + 31) / 32;
-    const long long tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b;
+    const long long tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b * NC;
     constexpr size_t smem = rd_smem_bytes<T, N>();
     static bool attr_set = false;
     if (!attr_set) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST>,
+        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
-    r2r_rd_kernel<T, N, AXIS, LD, ST><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
-        c.g, kind, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
+    r2r_rd_kernel<T, N, AXIS, LD, ST, NC><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+        c.g, kinds, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
     return SMADFT_OK;
@@ -244,9 +249,9 @@ int launch_axis(Ctx &c, int kind, LD ld, ST st)
     if constexpr (AXIS != 2) {
         if (c.use_rd) {
             switch (n) {
-            case 64: return launch_rd<T, 64, AXIS>(c, kind, ld, st);
-            case 128: return launch_rd<T, 128, AXIS>(c, kind, ld, st);
-            case 256: return launch_rd<T, 256, AXIS>(c, kind, ld, st);
+            case 64: return launch_rd<T, 64, AXIS>(c, KindSet<1>{{kind}}, ld, st);
+            case 128: return launch_rd<T, 128, AXIS>(c, KindSet<1>{{kind}}, ld, st);
+            case 256: return launch_rd<T, 256, AXIS>(c, KindSet<1>{{kind}}, ld, st);
             default: break;
             }
         }
@@ -372,6 +377,42 @@ int r2r3d(Ctx &c, int kx, int ky, int kz, LD ld, ST st)
     return launch_axis<T, 0>(c, kx, LoadArr<T>{tmp}, st);
 }
 
+// Runs fn(m) for m < n on forked streams: each branch starts after the work queued so far
+// and the stream continues after all branches.  Under stream capture the branches become
+// parallel paths of the graph, so the tails and launch gaps of independent passes overlap.
+template <class F>
+int forked(Ctx &c, int n, F fn)
+{
+    if (!c.use_fork || n <= 1 || !c.aux[0] || !c.ev_fork) {
+        for (int m = 0; m < n; m++)
+            if (int rc = fn(m)) return rc;
+        return SMADFT_OK;
+    }
+    const cudaStream_t main = c.stream;
+    cudaError_t e = cudaEventRecord(c.ev_fork, main);
+    int rc = SMADFT_OK;
+    for (int m = 0; m < n && e == cudaSuccess && rc == SMADFT_OK; m++) {
+        const cudaStream_t s = c.aux[m % Ctx::kMaxFork];
+        e = cudaStreamWaitEvent(s, c.ev_fork, 0);
+        if (e != cudaSuccess) break;
+        c.stream = s;
+        rc = fn(m);
+        c.stream = main;
+        e = cudaEventRecord(c.ev_join[m % Ctx::kMaxFork], s);
+    }
+    // join every branch that was started (also on error, so that a capture can end)
+    for (int m = 0; m < n && m < Ctx::kMaxFork; m++) {
+        const cudaError_t ej = cudaStreamWaitEvent(main, c.ev_join[m], 0);
+        if (e == cudaSuccess) e = ej;
+    }
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+        c.err = std::string("forked streams: ") + cudaGetErrorString(e);
+        return SMADFT_ERR_CUDA;
+    }
+    return SMADFT_OK;
+}
+
 // NC 3-D transforms whose loaders share input fields: component m goes from loader ls[m]
 // to field out[m] with kinds (kx[m], ky[m], kz[m]).  Plane path: one plane launch for all
 // components (their shared reads meet in L2), then the x pass of each in place; otherwise
@@ -390,9 +431,27 @@ int r2r3d_multi(Ctx &c, const int (&kx)[NC], const int (&ky)[NC], const int (&kz
             sm.p[m] = out[m];
         }
         if ((rc = launch_plane_n<T, NC>(c, pk, make_multi(ls...), sm))) return rc;
-        for (int m = 0; m < NC; m++)
-            if ((rc = launch_axis<T, 0>(c, kx[m], LoadArr<T>{out[m]}, StoreArr<T>{out[m]}))) return rc;
-        return rc;
+        return forked(c, NC, [&](int m) { return launch_axis<T, 0>(c, kx[m], LoadArr<T>{out[m]}, StoreArr<T>{out[m]}); });
+    }
+    if (c.use_rd && c.use_multi && (c.g.ny == 64 || c.g.ny == 128 || c.g.ny == 256)) {
+        // y pass of all components in one register-direct launch (their shared reads meet
+        // in L2), then the z and x passes of each in place
+        KindSet<NC> ks;
+        StoreMulti<T, NC> sm;
+        for (int m = 0; m < NC; m++) {
+            ks.k[m] = ky[m];
+            sm.p[m] = out[m];
+        }
+        switch (c.g.ny) {
+        case 64: rc = launch_rd<T, 64, 1>(c, ks, make_multi(ls...), sm); break;
+        case 128: rc = launch_rd<T, 128, 1>(c, ks, make_multi(ls...), sm); break;
+        default: rc = launch_rd<T, 256, 1>(c, ks, make_multi(ls...), sm); break;
+        }
+        if (rc) return rc;
+        return forked(c, NC, [&](int m) {
+            const int r = launch_axis<T, 2>(c, kz[m], LoadArr<T>{out[m]}, StoreArr<T>{out[m]});
+            return r ? r : launch_axis<T, 0>(c, kx[m], LoadArr<T>{out[m]}, StoreArr<T>{out[m]});
+        });
     }
     int m = 0;
     ((rc = rc ? rc : r2r3d<T>(c, kx[m], ky[m], kz[m], ls, StoreArr<T>{out[m]}), m++), ...);

@@ -294,13 +294,23 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
     T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
     int rc;
     // f', grad psi, grad rho (quasi/quasi.cpp:1121-1304)
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdDfd<T>{s, ph}, StoreArr<T>{dfd}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdGrad<T, 0>{s, ph}, StoreArr<T>{gx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdGrad<T, 1>{s, ph}, StoreArr<T>{gy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdGrad<T, 2>{s, ph}, StoreArr<T>{gz}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdGrad<T, 0>{s, rq}, StoreArr<T>{rx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdGrad<T, 1>{s, rq}, StoreArr<T>{ry}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdGrad<T, 2>{s, rq}, StoreArr<T>{rz}))) return rc;
+    {
+        const int kx[4] = {K_DCT3, K_DST3, K_DCT3, K_DCT3};
+        const int ky[4] = {K_DCT3, K_DCT3, K_DST3, K_DCT3};
+        const int kz[4] = {K_DCT3, K_DCT3, K_DCT3, K_DST3};
+        T *const out[4] = {dfd, gx, gy, gz};
+        if ((rc = r2r3d_multi<T, 4>(c, kx, ky, kz, out, LdDfd<T>{s, ph}, LdGrad<T, 0>{s, ph}, LdGrad<T, 1>{s, ph},
+                                    LdGrad<T, 2>{s, ph})))
+            return rc;
+    }
+    {
+        const int kx[3] = {K_DST3, K_DCT3, K_DCT3};
+        const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
+        const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
+        T *const out[3] = {rx, ry, rz};
+        if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdGrad<T, 0>{s, rq}, LdGrad<T, 1>{s, rq}, LdGrad<T, 2>{s, rq})))
+            return rc;
+    }
     // density law + filter (:1322-1357)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdRhoRaw<T>{psi, gx, gy, gz, s.kp, s.rho0, s.q02},
                        StFilter<T>{s, rq}))) return rc;
@@ -321,21 +331,29 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
     }
     SMADFT_CUDA(cudaMemcpyAsync(ro, rho, sizeof(T) * c.n, cudaMemcpyDeviceToDevice, c.stream));  // :1439
     // forces (:1448-1504); the x loader also stores mu and e
-    if ((rc = r2r3d<T>(c, K_DST2, K_DCT2, K_DCT2,
-                       LdQForce<T, 0>{psi, dfd, lap, rho, gx, rx, mu, en, s.eps, s.beta, s.gamma, lap_rho},
-                       StoreArr<T>{Sx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DST2, K_DCT2,
-                       LdQForce<T, 1>{psi, dfd, lap, rho, gy, ry, nullptr, nullptr, s.eps, s.beta, s.gamma, lap_rho},
-                       StoreArr<T>{Sy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DST2,
-                       LdQForce<T, 2>{psi, dfd, lap, rho, gz, rz, nullptr, nullptr, s.eps, s.beta, s.gamma, lap_rho},
-                       StoreArr<T>{Sz}))) return rc;
-    // pressure (:1510-1592)
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdPressure<T>{s, Sx, Sy, Sz, dv}, StoreArr<T>{pp}))) return rc;
-    // velocity = solenoidal + irrotational (:1599-2123)
-    if ((rc = r2r3d<T>(c, K_DST3, K_DCT3, K_DCT3, LdStokes<T, 0, true>{s, Sx, Sy, Sz, dv}, StoreArr<T>{vx}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DST3, K_DCT3, LdStokes<T, 1, true>{s, Sx, Sy, Sz, dv}, StoreArr<T>{vy}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DST3, LdStokes<T, 2, true>{s, Sx, Sy, Sz, dv}, StoreArr<T>{vz}))) return rc;
+    {
+        const int kx[3] = {K_DST2, K_DCT2, K_DCT2};
+        const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
+        const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
+        T *const out[3] = {Sx, Sy, Sz};
+        if ((rc = r2r3d_multi<T, 3>(
+                 c, kx, ky, kz, out,
+                 LdQForce<T, 0>{psi, dfd, lap, rho, gx, rx, mu, en, s.eps, s.beta, s.gamma, lap_rho},
+                 LdQForce<T, 1>{psi, dfd, lap, rho, gy, ry, nullptr, nullptr, s.eps, s.beta, s.gamma, lap_rho},
+                 LdQForce<T, 2>{psi, dfd, lap, rho, gz, rz, nullptr, nullptr, s.eps, s.beta, s.gamma, lap_rho})))
+            return rc;
+    }
+    // pressure (:1510-1592) and velocity = solenoidal + irrotational (:1599-2123)
+    {
+        const int kx[4] = {K_DCT3, K_DST3, K_DCT3, K_DCT3};
+        const int ky[4] = {K_DCT3, K_DCT3, K_DST3, K_DCT3};
+        const int kz[4] = {K_DCT3, K_DCT3, K_DCT3, K_DST3};
+        T *const out[4] = {pp, vx, vy, vz};
+        if ((rc = r2r3d_multi<T, 4>(c, kx, ky, kz, out, LdPressure<T>{s, Sx, Sy, Sz, dv},
+                                    LdStokes<T, 0, true>{s, Sx, Sy, Sz, dv}, LdStokes<T, 1, true>{s, Sx, Sy, Sz, dv},
+                                    LdStokes<T, 2, true>{s, Sx, Sy, Sz, dv})))
+            return rc;
+    }
     // N and the BDF2-like update (:2128-2182)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
                        LdQN<T>{mu, vx, vy, vz, gx, gy, gz, pp, rho, en, rx, ry, rz, s.kp,

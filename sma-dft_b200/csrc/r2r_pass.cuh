@@ -10,6 +10,8 @@
 // Passes are in place on the tile, so a 3-D transform needs one scratch field.
 #pragma once
 
+#include <type_traits>
+
 #include "fft_tile.cuh"
 
 namespace smadft {
@@ -123,6 +125,119 @@ struct StoreArr {
     template <int V>
     __device__ __forceinline__ void store(long long idx, int, int, int, const T *v) const { vst<T, V>(p, idx, v); }
 };
+
+// per-component kinds of the y and z transforms
+template <int NC>
+struct PlaneKinds {
+    int ky[NC], kz[NC];
+};
+
+// Loader / storer calls with a component index: multi-component functors (MULTI) take it,
+// single ones ignore it.
+template <class X, class = void>
+struct is_multi : std::false_type {};
+template <class X>
+struct is_multi<X, std::void_t<decltype(X::MULTI)>> : std::true_type {};
+
+// NC loaders behind one component index (the index is uniform over a CTA)
+template <class... L>
+struct LoadMulti;
+template <class L0>
+struct LoadMulti<L0> {
+    static constexpr bool MULTI = true;
+    L0 h;
+    template <int V, typename T>
+    __device__ __forceinline__ void load(int, long long q, int i, int j, int k, T *out) const
+    {
+        h.template load<V>(q, i, j, k, out);
+    }
+    // f(loader of component comp): the dispatch happens once, around a whole load loop
+    template <class F>
+    __device__ __forceinline__ void visit(int, F &&f) const { f(h); }
+};
+template <class L0, class L1, class... Ls>
+struct LoadMulti<L0, L1, Ls...> {
+    static constexpr bool MULTI = true;
+    L0 h;
+    LoadMulti<L1, Ls...> t;
+    template <int V, typename T>
+    __device__ __forceinline__ void load(int comp, long long q, int i, int j, int k, T *out) const
+    {
+        if (comp == 0) h.template load<V>(q, i, j, k, out);
+        else t.template load<V>(comp - 1, q, i, j, k, out);
+    }
+    template <class F>
+    __device__ __forceinline__ void visit(int comp, F &&f) const
+    {
+        if (comp == 0) f(h);
+        else t.visit(comp - 1, f);
+    }
+};
+
+// f(ld), or f(loader of component comp) for a multi-component loader
+template <class LD, class F>
+__device__ __forceinline__ void visit_c(const LD &ld, int comp, F &&f)
+{
+    if constexpr (is_multi<LD>::value) ld.visit(comp, f);
+    else f(ld);
+}
+template <class L0>
+LoadMulti<L0> make_multi(L0 a) { return LoadMulti<L0>{a}; }
+template <class L0, class L1, class... Ls>
+LoadMulti<L0, L1, Ls...> make_multi(L0 a, L1 b, Ls... r) { return LoadMulti<L0, L1, Ls...>{a, make_multi(b, r...)}; }
+
+// plain stores of component c into field p[c]
+template <typename T, int NC>
+struct StoreMulti {
+    static constexpr bool MULTI = true;
+    T *p[NC];
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(int, long long, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void fin(int comp, long long idx, int, int, int, const T *v, const T *) const
+    {
+        vst<T, V>(p[comp], idx, v);
+    }
+    template <int V>
+    __device__ __forceinline__ void store(int comp, long long idx, int, int, int, const T *v) const
+    {
+        vst<T, V>(p[comp], idx, v);
+    }
+};
+
+// per-component transform kind of a multi-component pass
+template <int NC>
+struct KindSet {
+    int k[NC];
+};
+
+template <int V, class LD, typename T>
+__device__ __forceinline__ void load_c(const LD &ld, int comp, long long q, int i, int j, int k, T *out)
+{
+    if constexpr (is_multi<LD>::value) ld.template load<V>(comp, q, i, j, k, out);
+    else ld.template load<V>(q, i, j, k, out);
+}
+template <int V, class ST, typename T>
+__device__ __forceinline__ void pre_c(const ST &st, int comp, long long q, int i, int j, int k, T *buf)
+{
+    if constexpr (is_multi<ST>::value) st.template pre<V>(comp, q, i, j, k, buf);
+    else st.template pre<V>(q, i, j, k, buf);
+}
+template <int V, class ST, typename T>
+__device__ __forceinline__ void fin_c(const ST &st, int comp, long long q, int i, int j, int k, const T *v,
+                                      const T *buf)
+{
+    if constexpr (is_multi<ST>::value) st.template fin<V>(comp, q, i, j, k, v, buf);
+    else st.template fin<V>(q, i, j, k, v, buf);
+}
+template <int V, class ST, typename T>
+__device__ __forceinline__ void store_c(const ST &st, int comp, long long q, int i, int j, int k, const T *v)
+{
+    if constexpr (is_multi<ST>::value) st.template store<V>(comp, q, i, j, k, v);
+    else st.template store<V>(q, i, j, k, v);
+}
+
 
 // buffer length for a storer's pre() values of V elements (at least 1)
 template <class ST, int V>

@@ -51,54 +51,6 @@ constexpr size_t plane_smem_bytes() { return plane_body_bytes<T, N>() + 2 * (siz
 
 __device__ __forceinline__ int plane_swz(int r) { return ((r >> 1) & 15) << 1; }
 
-// per-component kinds of the y and z transforms
-template <int NC>
-struct PlaneKinds {
-    int ky[NC], kz[NC];
-};
-
-// NC loaders behind one component index (the index is uniform over a CTA)
-template <class... L>
-struct LoadMulti;
-template <class L0>
-struct LoadMulti<L0> {
-    L0 h;
-    template <int V, typename T>
-    __device__ __forceinline__ void load(int, long long q, int i, int j, int k, T *out) const
-    {
-        h.template load<V>(q, i, j, k, out);
-    }
-};
-template <class L0, class L1, class... Ls>
-struct LoadMulti<L0, L1, Ls...> {
-    L0 h;
-    LoadMulti<L1, Ls...> t;
-    template <int V, typename T>
-    __device__ __forceinline__ void load(int comp, long long q, int i, int j, int k, T *out) const
-    {
-        if (comp == 0) h.template load<V>(q, i, j, k, out);
-        else t.template load<V>(comp - 1, q, i, j, k, out);
-    }
-};
-template <class L0>
-LoadMulti<L0> make_multi(L0 a) { return LoadMulti<L0>{a}; }
-template <class L0, class L1, class... Ls>
-LoadMulti<L0, L1, Ls...> make_multi(L0 a, L1 b, Ls... r) { return LoadMulti<L0, L1, Ls...>{a, make_multi(b, r...)}; }
-
-// plain stores of component c into field p[c]
-template <typename T, int NC>
-struct StoreMulti {
-    T *p[NC];
-    static constexpr int PRE = 0;
-    template <int V>
-    __device__ __forceinline__ void pre(int, long long, int, int, int, T *) const {}
-    template <int V>
-    __device__ __forceinline__ void fin(int comp, long long idx, int, int, int, const T *v, const T *) const
-    {
-        vst<T, V>(p[comp], idx, v);
-    }
-};
-
 // one packed pair (k, k + 1) of a row; p is 2 sizeof(T)-aligned
 template <typename T>
 __device__ __forceinline__ cpx<T> ld_pair(const T *p)
@@ -150,15 +102,17 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_plane_kernel(Geom g
         const int r0 = rank * ROWS;
         constexpr int PER = kRdLines * (N / 2) / NT;      // (line, sample pair) tasks per thread
         T va[PER][2], vb[PER][2];
+        ld.visit(comp, [&](const auto &l) {
 #pragma unroll
-        for (int e = 0; e < PER; e++) {
-            const int t = e * NT + threadIdx.x;
-            const int ln = t / (N / 2), n = 2 * (t % (N / 2));
-            const int ja = r0 + 2 * ln;
-            const long long qa = pbase + (long long)ja * g.nz + n;
-            ld.template load<2>(comp, qa, i, ja, n, va[e]);
-            ld.template load<2>(comp, qa + g.nz, i, ja + 1, n, vb[e]);
-        }
+            for (int e = 0; e < PER; e++) {
+                const int t = e * NT + threadIdx.x;
+                const int ln = t / (N / 2), n = 2 * (t % (N / 2));
+                const int ja = r0 + 2 * ln;
+                const long long qa = pbase + (long long)ja * g.nz + n;
+                l.template load<2>(qa, i, ja, n, va[e]);
+                l.template load<2>(qa + g.nz, i, ja + 1, n, vb[e]);
+            }
+        });
 #pragma unroll
         for (int e = 0; e < PER; e++) {
             const int t = e * NT + threadIdx.x;

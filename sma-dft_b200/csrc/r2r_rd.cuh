@@ -289,8 +289,10 @@ __device__ __forceinline__ int rd_out_pos(int j, int pnt, bool fwd, bool sine)
     return kk < N / 2 ? 2 * kk : 2 * (N - 1 - kk) + 1;
 }
 
-template <typename T, int N, int AXIS, class LD, class ST>
-__global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2r_rd_kernel(Geom g, int kind, int tiles_b, LD ld,
+// NC > 1: multi-component pass (LoadMulti / StoreMulti); CTA b transforms component b mod NC
+// of tile b / NC, so the components' shared input reads meet in L2.
+template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2r_rd_kernel(Geom g, KindSet<NC> kinds, int tiles_b, LD ld,
                                                                        const cpx<T> *__restrict__ wt_g,
                                                                        const cpx<T> *__restrict__ ht_g, ST st)
 {
@@ -314,8 +316,11 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     const int c = lane & 15;
     const int j = (wi == 0) ? (hh16 ? R1 / 2 : 0) : (hh16 ? R1 - wi : wi);
     // tile: 32 k-columns starting at kt*32 along the non-transformed line coordinate `a`
-    const int kt = blockIdx.x % tiles_b;
-    const int a = blockIdx.x / tiles_b;
+    const int comp = NC > 1 ? (int)(blockIdx.x % NC) : 0;
+    const int bt = NC > 1 ? (int)(blockIdx.x / NC) : (int)blockIdx.x;
+    const int kind = kinds.k[comp];
+    const int kt = bt % tiles_b;
+    const int a = bt / tiles_b;
     const int k = kt * 32 + 2 * c;                 // first of the two real lines
     const long long stride = AXIS == 1 ? (long long)g.nz : g.nyz;
     const long long base = (AXIS == 1 ? (long long)a * g.nyz : (long long)a * g.nz) + k;
@@ -327,12 +332,12 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
 
     // the pair of real samples (lines k, k+1) at line position t, packed as one complex;
     // the Loader computes them from its fields (each point is loaded exactly once)
-    auto load_pair = [&](int t, bool edge) -> cpx<T> {
+    auto load_pair = [&](const auto &l, int t, bool edge) -> cpx<T> {
         const long long q = base + (long long)t * stride;
         const int ii = AXIS == 1 ? a : t, jj = AXIS == 1 ? t : a;
         T v[2] = {T(0), T(0)};
-        if (!edge || nk >= 2) ld.template load<2>(q, ii, jj, k, v);
-        else if (nk == 1) ld.template load<1>(q, ii, jj, k, v);
+        if (!edge || nk >= 2) l.template load<2>(q, ii, jj, k, v);
+        else if (nk == 1) l.template load<1>(q, ii, jj, k, v);
         return {v[0], v[1]};
     };
     auto src_pos = [&](int q) -> int {       // natural line position of stage-0 point q
@@ -342,13 +347,16 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     };
 
     cpx<T> v[R0];
-    if (full) {
+    // one straight-line load loop per loader (a multi-component loader is resolved once per CTA)
+    visit_c(ld, comp, [&](const auto &l) {
+        if (full) {
 #pragma unroll
-        for (int q = 0; q < R0; q++) v[q] = load_pair(src_pos(q), false);
-    } else {
+            for (int q = 0; q < R0; q++) v[q] = load_pair(l, src_pos(q), false);
+        } else {
 #pragma unroll
-        for (int q = 0; q < R0; q++) v[q] = load_pair(src_pos(q), true);
-    }
+            for (int q = 0; q < R0; q++) v[q] = load_pair(l, src_pos(q), true);
+        }
+    });
     if (fwd) {
         // Makhoul-permuted input: DST-II negates odd natural samples
         if (sine) {
@@ -370,8 +378,8 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
         const long long q = base + (long long)o * stride;
         const int ii = AXIS == 1 ? a : o, jj = AXIS == 1 ? o : a;
         const T w2[2] = {z.x, z.y};
-        if (!edge || nk >= 2) st.template fin<2>(q, ii, jj, k, w2, pre_buf);
-        else if (nk == 1) st.template store<1>(q, ii, jj, k, w2);
+        if (!edge || nk >= 2) fin_c<2>(st, comp, q, ii, jj, k, w2, pre_buf);
+        else if (nk == 1) store_c<1>(st, comp, q, ii, jj, k, w2);
     };
     if (full) {
 #pragma unroll
@@ -380,7 +388,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
 #pragma unroll
             for (int u = 0; u < CH; u++) {
                 const int o = out_row(p0 + u);
-                st.template pre<2>(base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
+                pre_c<2>(st, comp, base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
             }
 #pragma unroll
             for (int u = 0; u < CH; u++) put(p0 + u, false, pre_buf[u]);
@@ -390,7 +398,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
         for (int p0 = 0; p0 < NP; p0++) {
             T pre_buf[PL];
             const int o = out_row(p0);
-            if (nk >= 2) st.template pre<2>(base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
+            if (nk >= 2) pre_c<2>(st, comp, base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
             put(p0, true, pre_buf);
         }
     }

@@ -350,9 +350,16 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     // the separate axis passes are the default (faster in FP32 on B200)
     if (const char *e = std::getenv("SMADFT_PLANE")) c.use_plane = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_RDZ")) c.use_rdz = e[0] != '0';
+    if (const char *e = std::getenv("SMADFT_MULTI")) c.use_multi = e[0] != '0';
+    if (const char *e = std::getenv("SMADFT_FORK")) c.use_fork = e[0] != '0';
     auto bail = [&](int code) { smadft_destroy(h); return code; };
     if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+    for (int m = 0; m < Ctx::kMaxFork; m++) {
+        if (cudaStreamCreateWithFlags(&c.aux[m], cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+        if (cudaEventCreateWithFlags(&c.ev_join[m], cudaEventDisableTiming) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+    }
+    if (cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
     for (int s : slots_for(p->model)) {
         if (cudaMalloc(&c.slot[s], c.esize * c.n) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
         if (cudaMemset(c.slot[s], 0, c.esize * c.n) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
@@ -382,6 +389,11 @@ int smadft_destroy(smadft_ctx *h)
     if (c.red) cudaFree(c.red);
     if (c.red_out) cudaFree(c.red_out);
     if (c.stage) cudaFree(c.stage);
+    for (int m = 0; m < Ctx::kMaxFork; m++) {
+        if (c.aux[m]) cudaStreamDestroy(c.aux[m]);
+        if (c.ev_join[m]) cudaEventDestroy(c.ev_join[m]);
+    }
+    if (c.ev_fork) cudaEventDestroy(c.ev_fork);
     if (c.stream) cudaStreamDestroy(c.stream);
     cudaGetLastError();
     delete h;

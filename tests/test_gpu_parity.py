@@ -132,9 +132,12 @@ def test_fp64_matches_oracle_fields(model, shape, steps, kw):
     (smadft.ADV, (12, 64, 64), 10, dict(dt=0.02)),
     (smadft.QUASI, (8, 64, 64), 8, dict(dt=0.002, kp=0.3755, divv_switch=4)),
 ])
-def test_plane_path_matches_oracle(model, shape, steps, kw, monkeypatch):
-    """The opt-in fused z + y plane kernel (SMADFT_PLANE=1, ny = nz = 64) through whole steps."""
-    monkeypatch.setenv("SMADFT_PLANE", "1")
+@pytest.mark.parametrize("plane", ["1", "0"], ids=["plane", "multi_y"])
+def test_ny64_paths_match_oracle(model, shape, steps, kw, plane, monkeypatch):
+    """ny = nz = 64 through whole steps: the opt-in fused z + y plane kernel (SMADFT_PLANE=1)
+    and the default separate passes, whose y pass runs the grouped transforms as one
+    multi-component register-direct launch."""
+    monkeypatch.setenv("SMADFT_PLANE", plane)
     p = smadft.params(model, shape, **kw)
     psi0 = smadft.ic_conics(p, A=1.3, count=2, rmin=1.0, rmax=2.0, noise=1e-3, seed=5)
     okw = dict(nw=p.nw, dt=p.dt, eps=p.eps, nu=p.nu, kp=p.kp, rho0=p.rho0, divv_switch=p.divv_switch)
