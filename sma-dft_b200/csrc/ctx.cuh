@@ -69,6 +69,8 @@ struct Ctx {
     size_t esize = 8;
     void *tables = nullptr;     // qx qy qz sx sy sz ex ey ez (T), contiguous
     size_t off[9] = {};
+    void *tables64 = nullptr;   // the same in FP64 (= tables for FP64 contexts): time-update coefficients
+    size_t off64[9] = {};
     std::map<int, PlanDev> plans;
     double *red = nullptr;      // reduction partials (device)
     double *red_out = nullptr;  // final sums (device)
@@ -110,9 +112,16 @@ template <typename T>
 Spec<T> make_spec(const Ctx &c)
 {
     Spec<T> s;
-    s.qx = c.tab<T>(0); s.qy = c.tab<T>(1); s.qz = c.tab<T>(2);
-    s.sx = c.tab<T>(3); s.sy = c.tab<T>(4); s.sz = c.tab<T>(5);
-    s.ex = c.tab<T>(6); s.ey = c.tab<T>(7); s.ez = c.tab<T>(8);
+    if constexpr (sizeof(T) == 8) {
+        // FP64 tables exist for every context (the time update always runs in FP64)
+        auto t = [&](int w) { return reinterpret_cast<const T *>(reinterpret_cast<const char *>(c.tables64) + c.off64[w]); };
+        s.qx = t(0); s.qy = t(1); s.qz = t(2); s.sx = t(3); s.sy = t(4); s.sz = t(5);
+        s.ex = t(6); s.ey = t(7); s.ez = t(8);
+    } else {
+        s.qx = c.tab<T>(0); s.qy = c.tab<T>(1); s.qz = c.tab<T>(2);
+        s.sx = c.tab<T>(3); s.sy = c.tab<T>(4); s.sz = c.tab<T>(5);
+        s.ex = c.tab<T>(6); s.ey = c.tab<T>(7); s.ez = c.tab<T>(8);
+    }
     const smadft_params &p = c.p;
     s.eps = T(p.eps); s.alpha = T(p.alpha); s.beta = T(p.beta); s.gamma = T(p.gamma);
     s.q02 = T(p.q0 * p.q0); s.dtd2 = T(p.dt / 2); s.dt = T(p.dt); s.scale = T(c.scale);
@@ -223,7 +232,7 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
     const PlanDev &pd = c.plans.at(N);
     const long long rows = (long long)c.g.nx * c.g.ny;
     const long long tiles = (rows + 2 * kRdLines - 1) / (2 * kRdLines);
-    constexpr size_t smem = rd_smem_bytes<T, N>();
+    constexpr size_t smem = rdz_smem_bytes<T, N>();
     static bool attr_set = false;
     if (!attr_set) {
         SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -222,9 +222,11 @@ struct LdAdvN {
 // Crank-Nicolson / Adams-Bashforth update fed by the freshly transformed N
 // (no-adv/cosNoAdvTrackSing.cpp:752-753, adv/cosAdvTrackMult.cpp:1362-1364):
 //   psihat <- (C1 psihat + dt/2 scale (3 N - Nprev)) / C2,  C1,2 = 1 +- dt/2 L(q);  Nprev <- N
+// The update runs in FP64 from FP64 wavenumbers for every field precision: C1/C2 is applied
+// to psihat every step, so a rounding error in it would grow linearly with the step count.
 template <typename T>
 struct StUpdCN {
-    Spec<T> s;
+    Spec<double> s;
     T *__restrict__ ph;
     T *__restrict__ np;
     static constexpr int PRE = 2;   // psihat, Nprev
@@ -240,9 +242,9 @@ struct StUpdCN {
         T o[V];
 #pragma unroll
         for (int u = 0; u < V; u++) {
-            const T al = s.alin(i, j, k + u);
-            const T c1 = T(1) + s.dtd2 * al, c2 = T(1) - s.dtd2 * al;
-            o[u] = (c1 * buf[u] + s.dtd2 * s.scale * (T(3) * v[u] - buf[V + u])) / c2;
+            const double al = s.alin(i, j, k + u);
+            const double c1 = 1.0 + s.dtd2 * al, c2 = 1.0 - s.dtd2 * al;
+            o[u] = T((c1 * double(buf[u]) + s.dtd2 * s.scale * (3.0 * double(v[u]) - double(buf[V + u]))) / c2);
         }
         vst<T, V>(ph, q, o);
         vst<T, V>(np, q, v);

@@ -229,9 +229,10 @@ struct LdQN {
 
 // psihat <- (C1 psihat - psihat_old/2 + dt/2 scale (3 N - Nprev)) / C2,
 // C1 = 2 - dt rho_m L, C2 = 1.5 - dt rho_m L; first step uses Nprev = N (quasi/quasi.cpp:2162-2182)
+// Runs in FP64 for every field precision (see StUpdCN).
 template <typename T>
 struct StUpdBDF {
-    Spec<T> s;
+    Spec<double> s;
     T *__restrict__ ph, *__restrict__ pho, *__restrict__ np;
     int first;
     static constexpr int PRE = 3;   // psihat, psihat_old, Nprev
@@ -248,10 +249,10 @@ struct StUpdBDF {
         T o[V];
 #pragma unroll
         for (int u = 0; u < V; u++) {
-            const T al = s.alin(i, j, k + u);
-            const T c1 = T(2) - s.dt * s.rho_m * al, c2 = T(1.5) - s.dt * s.rho_m * al;
-            const T npv = first ? v[u] : buf[2 * V + u];
-            o[u] = (c1 * buf[u] - T(0.5) * buf[V + u] + s.dtd2 * s.scale * (T(3) * v[u] - npv)) / c2;
+            const double al = s.alin(i, j, k + u);
+            const double c1 = 2.0 - s.dt * s.rho_m * al, c2 = 1.5 - s.dt * s.rho_m * al;
+            const double npv = first ? double(v[u]) : double(buf[2 * V + u]);
+            o[u] = T((c1 * double(buf[u]) - 0.5 * double(buf[V + u]) + s.dtd2 * s.scale * (3.0 * double(v[u]) - npv)) / c2);
         }
         vst<T, V>(ph, q, o);
         vst<T, V>(pho, q, buf);
@@ -358,7 +359,7 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
                        LdQN<T>{mu, vx, vy, vz, gx, gy, gz, pp, rho, en, rx, ry, rz, s.kp,
                                (int)(nloop > P.divv_switch + 1)},
-                       StUpdBDF<T>{s, ph, pho, np, (int)(nloop == 1)}))) return rc;
+                       StUpdBDF<T>{make_spec<double>(c), ph, pho, np, (int)(nloop == 1)}))) return rc;
     // psi = iCT(psihat) (:2186-2190)
     T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
     return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{dst});

@@ -69,7 +69,7 @@ __device__ __forceinline__ void rd_fft(cpx<T> (&v)[RdInfo<N>::R0],
                                        cpx<T> (&x1)[RdInfo<N>::R0 / RdInfo<N>::R1 > 0 ? RdInfo<N>::R0 / RdInfo<N>::R1 : 1]
                                                    [RdInfo<N>::R1],
                                        cpx<T> *line, const cpx<T> *wt, const cpx<T> *ht, int j, int wi, bool fwd,
-                                       bool sine)
+                                       bool sine, const cpx<T> *wz = nullptr)
 {
     using RI = RdInfo<N>;
     constexpr int R0 = RI::R0, R1 = RI::R1;
@@ -155,7 +155,11 @@ __device__ __forceinline__ void rd_fft(cpx<T> (&v)[RdInfo<N>::R0],
 #pragma unroll
     for (int q = 0; q < R0; q++) {
         cpx<T> o = v[q];
-        if (q > 0) o = fwd ? cmul(o, tw<T, false>(wt, j * q)) : cmul(o, tw<T, true>(wt, j * q));
+        // ZMAP reads W_N^(j q) from the transposed table wz[q R1 + j] (consecutive lanes,
+        // consecutive banks); the strided layout broadcasts wt[j q] over a half-warp
+        const cpx<T> *wq = ZMAP ? wz : wt;
+        const int e = ZMAP ? q * R1 + j : j * q;
+        if (q > 0) o = fwd ? cmul(o, tw<T, false>(wq, e)) : cmul(o, tw<T, true>(wq, e));
         line[RI::phys(j + q * R1)] = o;
     }
     __syncthreads();

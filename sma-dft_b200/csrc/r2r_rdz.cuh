@@ -19,6 +19,9 @@
 
 namespace smadft {
 
+template <typename T, int N>
+constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * sizeof(cpx<T>); }
+
 // rows = number of z lines (nx * ny); a CTA transforms 2 * kRdLines consecutive rows
 template <typename T, int N>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(long long rows, int kind, const T *in, T *out,
@@ -33,9 +36,11 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     cpx<T> *buf = reinterpret_cast<cpx<T> *>(smem_raw);
     cpx<T> *wt = buf + kRdLines * RI::LD;
     cpx<T> *ht = wt + N;
+    cpx<T> *wz = ht + N;                            // stage-0 twiddles W_N^(j q) at q R1 + j
     for (int m = threadIdx.x; m < N; m += NT) {
         wt[m] = wt_g[m];
         ht[m] = ht_g[m];
+        wz[m] = wt_g[(m % R1) * (m / R1)];
     }
     const int j = threadIdx.x % R1;                 // first-stage butterfly (lane in its group)
     const int c = threadIdx.x / R1;                 // complex line of the CTA
@@ -61,7 +66,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     }
     __syncthreads();                                 // twiddle tables
     cpx<T> x1[BPT][R1];
-    rd_fft<T, N, true>(v, x1, buf + c * RI::LD, wt, ht, j, threadIdx.x >> 5, fwd, sine);
+    rd_fft<T, N, true>(v, x1, buf + c * RI::LD, wt, ht, j, threadIdx.x >> 5, fwd, sine, wz);
 #pragma unroll
     for (int pnt = 0; pnt < NP; pnt++) {
         const cpx<T> z = x1[pnt / R1][pnt % R1];

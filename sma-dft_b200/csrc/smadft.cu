@@ -105,6 +105,18 @@ int upload_tables(Ctx &c)
     }
     SMADFT_CUDA(cudaMalloc(&c.tables, all.size() * sizeof(T)));
     SMADFT_CUDA(cudaMemcpy(c.tables, all.data(), all.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (sizeof(T) == 8) {
+        c.tables64 = c.tables;
+        for (int q = 0; q < 9; q++) c.off64[q] = c.off[q];
+    } else {
+        std::vector<double> all64;
+        for (int q = 0; q < 9; q++) {
+            c.off64[q] = all64.size() * sizeof(double);
+            for (double v : *t[q]) all64.push_back(v);
+        }
+        SMADFT_CUDA(cudaMalloc(&c.tables64, all64.size() * sizeof(double)));
+        SMADFT_CUDA(cudaMemcpy(c.tables64, all64.data(), all64.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     return SMADFT_OK;
 }
 
@@ -385,6 +397,7 @@ int smadft_destroy(smadft_ctx *h)
     for (int s = 0; s < S_COUNT; s++)
         if (c.slot[s]) cudaFree(c.slot[s]);
     for (auto &kv : c.plans) { cudaFree(kv.second.w); cudaFree(kv.second.h); }
+    if (c.tables64 && c.tables64 != c.tables) cudaFree(c.tables64);
     if (c.tables) cudaFree(c.tables);
     if (c.red) cudaFree(c.red);
     if (c.red_out) cudaFree(c.red_out);

@@ -47,7 +47,7 @@ int adv_step(Ctx &c)
     }
     // N = beta psi^3 - gamma psi^5 - v.grad psi, CN/AB2 update (:1290-1365)
     return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
-                    LdAdvN<T>{psi, vx, vy, vz, gx, gy, gz, s.beta, s.gamma}, StUpdCN<T>{s, ph, np});
+                    LdAdvN<T>{psi, vx, vy, vz, gx, gy, gz, s.beta, s.gamma}, StUpdCN<T>{make_spec<double>(c), ph, np});
 }
 
 // each precision builds as its own object (SMADFT_INST_FLOAT / SMADFT_INST_DOUBLE); a plain

@@ -12,7 +12,7 @@ int noadv_step(Ctx &c, bool keep_old)
     T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
     // N^n = REDFT10^3(beta psi^3 - gamma psi^5), fused CN/AB2 update of psihat
     int rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
-                      StUpdCN<T>{s, ph, np});
+                      StUpdCN<T>{make_spec<double>(c), ph, np});
     if (rc) return rc;
     // psi^{n+1} = REDFT01^3 psihat (into the second buffer when the old psi is needed)
     T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
