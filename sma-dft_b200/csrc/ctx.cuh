@@ -28,6 +28,11 @@ enum Slot : int {
     S_COUNT
 };
 
+// The spectral state psihat (and quasi's psihat_old) is FP64 in every context: it carries
+// the run from step to step, so its rounding would accumulate.  Nprev only enters the
+// AB2 extrapolation and is replaced every step: it stays in the field precision.
+inline bool slot_is_state(int s) { return s == S_PSIH || s == S_PSIH_OLD; }
+
 struct PlanDev {
     int nst;
     int radix[kMaxStages];

@@ -52,10 +52,10 @@ struct LdNonlin {
 // Index-shifted gradient spectra (adv/cosAdvTrackMult.cpp:904-959): G_c = -s_c f[+1 along c],
 // zero at the last index of c.  Branch-free: out-of-range points read a clamped in-range
 // address and are zeroed by a select, so the loads of all points can be issued together.
-template <typename T, int AX>
+template <typename T, int AX, typename S = T>
 struct LdGrad {
     Spec<T> s;
-    const T *__restrict__ f;
+    const S *__restrict__ f;
     template <int V>
     __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
@@ -63,7 +63,7 @@ struct LdGrad {
             const bool in = AX == 0 ? (i < s.nx - 1) : (j < s.ny - 1);
             const long long sh = AX == 0 ? s.nyz : (long long)s.nz;
             T v[V];
-            vld<T, V>(f, in ? q + sh : q, v);
+            vld_as<T, V, S>(f, in ? q + sh : q, v);
             const T sc = in ? -(AX == 0 ? s.sx[i] : s.sy[j]) : T(0);
 #pragma unroll
             for (int u = 0; u < V; u++) out[u] = sc * v[u];
@@ -71,7 +71,7 @@ struct LdGrad {
 #pragma unroll
             for (int u = 0; u < V; u++) {
                 const bool in = k + u < s.nz - 1;
-                const T x = f[in ? q + u + 1 : q + u];
+                const T x = T(f[in ? q + u + 1 : q + u]);
                 out[u] = in ? -s.sz[k + u] * x : T(0);
             }
         }
@@ -82,12 +82,12 @@ struct LdGrad {
 template <typename T>
 struct LdNegLin {
     Spec<T> s;
-    const T *__restrict__ ph;
+    const double *__restrict__ ph;   // spectral state (FP64)
     template <int V>
     __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
         T v[V];
-        vld<T, V>(ph, q, v);
+        vld_as<T, V, double>(ph, q, v);
 #pragma unroll
         for (int u = 0; u < V; u++) out[u] = -s.alin(i, j, k + u) * v[u];
     }
@@ -227,32 +227,33 @@ struct LdAdvN {
 template <typename T>
 struct StUpdCN {
     Spec<double> s;
-    T *__restrict__ ph;
-    T *__restrict__ np;
+    double *__restrict__ ph;        // spectral state (FP64 for every compute precision)
+    T *__restrict__ np;             // Nprev (field precision)
     static constexpr int PRE = 2;   // psihat, Nprev
+    using Pre = double;
     template <int V>
-    __device__ __forceinline__ void pre(long long q, int, int, int, T *buf) const
+    __device__ __forceinline__ void pre(long long q, int, int, int, double *buf) const
     {
-        vld<T, V>(ph, q, buf);
-        vld<T, V>(np, q, buf + V);
+        vld<double, V>(ph, q, buf);
+        vld_as<double, V, T>(np, q, buf + V);
     }
     template <int V>
-    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *buf) const
+    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const double *buf) const
     {
-        T o[V];
+        double o[V];
 #pragma unroll
         for (int u = 0; u < V; u++) {
             const double al = s.alin(i, j, k + u);
             const double c1 = 1.0 + s.dtd2 * al, c2 = 1.0 - s.dtd2 * al;
-            o[u] = T((c1 * double(buf[u]) + s.dtd2 * s.scale * (3.0 * double(v[u]) - double(buf[V + u]))) / c2);
+            o[u] = (c1 * buf[u] + s.dtd2 * s.scale * (3.0 * double(v[u]) - buf[V + u])) / c2;
         }
-        vst<T, V>(ph, q, o);
+        vst<double, V>(ph, q, o);
         vst<T, V>(np, q, v);
     }
     template <int V>
     __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
-        T buf[2 * V];
+        double buf[2 * V];
         pre<V>(q, i, j, k, buf);
         fin<V>(q, i, j, k, v, buf);
     }
@@ -261,8 +262,8 @@ struct StUpdCN {
 // Scales a forward transform into psihat (pre-loop: psihat = scale REDFT10^3 psi)
 template <typename T>
 struct StScale {
-    T *__restrict__ p;
-    T scale;
+    double *__restrict__ p;         // spectral state (FP64)
+    double scale;
     static constexpr int PRE = 0;
     template <int V>
     __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
@@ -274,10 +275,10 @@ struct StScale {
     template <int V>
     __device__ __forceinline__ void store(long long q, int, int, int, const T *v) const
     {
-        T o[V];
+        double o[V];
 #pragma unroll
-        for (int u = 0; u < V; u++) o[u] = scale * v[u];
-        vst<T, V>(p, q, o);
+        for (int u = 0; u < V; u++) o[u] = scale * double(v[u]);
+        vst<double, V>(p, q, o);
     }
 };
 

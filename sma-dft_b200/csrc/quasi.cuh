@@ -13,12 +13,12 @@ namespace smadft {
 template <typename T>
 struct LdDfd {
     Spec<T> s;
-    const T *__restrict__ ph;
+    const double *__restrict__ ph;   // spectral state (FP64)
     template <int V>
     __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
         T v[V];
-        vld<T, V>(ph, q, v);
+        vld_as<T, V, double>(ph, q, v);
 #pragma unroll
         for (int u = 0; u < V; u++) out[u] = s.alpha * (s.q02 - s.mq2(i, j, k + u)) * v[u];
     }
@@ -28,12 +28,12 @@ struct LdDfd {
 template <typename T>
 struct LdLapDfd {
     Spec<T> s;
-    const T *__restrict__ ph;
+    const double *__restrict__ ph;   // spectral state (FP64)
     template <int V>
     __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
     {
         T v[V];
-        vld<T, V>(ph, q, v);
+        vld_as<T, V, double>(ph, q, v);
 #pragma unroll
         for (int u = 0; u < V; u++) {
             const T m = s.mq2(i, j, k + u);
@@ -233,35 +233,38 @@ struct LdQN {
 template <typename T>
 struct StUpdBDF {
     Spec<double> s;
-    T *__restrict__ ph, *__restrict__ pho, *__restrict__ np;
+    double *__restrict__ ph, *__restrict__ pho;   // spectral state (FP64)
+    T *__restrict__ np;                           // Nprev (field precision)
     int first;
     static constexpr int PRE = 3;   // psihat, psihat_old, Nprev
+    using Pre = double;
     template <int V>
-    __device__ __forceinline__ void pre(long long q, int, int, int, T *buf) const
+    __device__ __forceinline__ void pre(long long q, int, int, int, double *buf) const
     {
-        vld<T, V>(ph, q, buf);
-        vld<T, V>(pho, q, buf + V);
-        vld<T, V>(np, q, buf + 2 * V);
+        vld<double, V>(ph, q, buf);
+        vld<double, V>(pho, q, buf + V);
+        vld_as<double, V, T>(np, q, buf + 2 * V);
     }
     template <int V>
-    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *buf) const
+    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const double *buf) const
     {
-        T o[V];
+        double o[V];
 #pragma unroll
         for (int u = 0; u < V; u++) {
             const double al = s.alin(i, j, k + u);
             const double c1 = 2.0 - s.dt * s.rho_m * al, c2 = 1.5 - s.dt * s.rho_m * al;
-            const double npv = first ? double(v[u]) : double(buf[2 * V + u]);
-            o[u] = T((c1 * double(buf[u]) - 0.5 * double(buf[V + u]) + s.dtd2 * s.scale * (3.0 * double(v[u]) - npv)) / c2);
+            const double nv = double(v[u]);
+            const double npv = first ? nv : buf[2 * V + u];
+            o[u] = (c1 * buf[u] - 0.5 * buf[V + u] + s.dtd2 * s.scale * (3.0 * nv - npv)) / c2;
         }
-        vst<T, V>(ph, q, o);
-        vst<T, V>(pho, q, buf);
+        vst<double, V>(ph, q, o);
+        vst<double, V>(pho, q, buf);
         vst<T, V>(np, q, v);
     }
     template <int V>
     __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
     {
-        T buf[3 * V];
+        double buf[3 * V];
         pre<V>(q, i, j, k, buf);
         fin<V>(q, i, j, k, v, buf);
     }
@@ -271,12 +274,13 @@ template <typename T>
 int quasi_pre_loop(Ctx &c)
 {
     Spec<T> s = make_spec<T>(c);
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH);
+    T *psi = c.f<T>(S_PSI);
+    double *ph = c.f<double>(S_PSIH);   // spectral state (FP64)
     int rc;
     // psihat = scale CT(psi); psi = iCT(psihat); psihat_old = psihat (quasi/quasi.cpp:990-1034)
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, s.scale}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{psi}))) return rc;
-    SMADFT_CUDA(cudaMemcpyAsync(c.slot[S_PSIH_OLD], ph, sizeof(T) * c.n, cudaMemcpyDeviceToDevice, c.stream));
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, c.scale}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T, double>{ph}, StoreArr<T>{psi}))) return rc;
+    SMADFT_CUDA(cudaMemcpyAsync(c.slot[S_PSIH_OLD], ph, sizeof(double) * c.n, cudaMemcpyDeviceToDevice, c.stream));
     return SMADFT_OK;
 }
 
@@ -285,7 +289,9 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
 {
     Spec<T> s = make_spec<T>(c);
     const smadft_params &P = c.p;
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *pho = c.f<T>(S_PSIH_OLD), *np = c.f<T>(S_NP);
+    T *psi = c.f<T>(S_PSI);
+    double *ph = c.f<double>(S_PSIH), *pho = c.f<double>(S_PSIH_OLD);   // FP64 state
+    T *np = c.f<T>(S_NP);
     T *gx = c.f<T>(S_GX), *gy = c.f<T>(S_GY), *gz = c.f<T>(S_GZ);
     T *rx = c.f<T>(S_RDX), *ry = c.f<T>(S_RDY), *rz = c.f<T>(S_RDZ);
     T *rho = c.f<T>(S_RHO), *ro = c.f<T>(S_RHO_OLD), *rq = c.f<T>(S_RHOQ);
@@ -300,8 +306,8 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
         const int ky[4] = {K_DCT3, K_DCT3, K_DST3, K_DCT3};
         const int kz[4] = {K_DCT3, K_DCT3, K_DCT3, K_DST3};
         T *const out[4] = {dfd, gx, gy, gz};
-        if ((rc = r2r3d_multi<T, 4>(c, kx, ky, kz, out, LdDfd<T>{s, ph}, LdGrad<T, 0>{s, ph}, LdGrad<T, 1>{s, ph},
-                                    LdGrad<T, 2>{s, ph})))
+        if ((rc = r2r3d_multi<T, 4>(c, kx, ky, kz, out, LdDfd<T>{s, ph}, LdGrad<T, 0, double>{s, ph},
+                                    LdGrad<T, 1, double>{s, ph}, LdGrad<T, 2, double>{s, ph})))
             return rc;
     }
     {
@@ -362,7 +368,7 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
                        StUpdBDF<T>{make_spec<double>(c), ph, pho, np, (int)(nloop == 1)}))) return rc;
     // psi = iCT(psihat) (:2186-2190)
     T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
-    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{dst});
+    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T, double>{ph}, StoreArr<T>{dst});
 }
 
 template <typename T>

@@ -102,29 +102,74 @@ __device__ __forceinline__ void vst(T *__restrict__ p, long long idx, const T *v
     }
 }
 
+// V elements of an array of element type S, converted to / from the compute type T (the
+// spectral state is FP64 for every compute precision); S == T is vld / vst.
+template <typename T, int V, typename S>
+__device__ __forceinline__ void vld_as(const S *__restrict__ p, long long idx, T *o)
+{
+    if constexpr (std::is_same<S, T>::value) {
+        vld<T, V>(p, idx, o);
+    } else {
+        S t[V];
+        if constexpr (sizeof(S) == 8 && V % 2 == 0) {
+#pragma unroll
+            for (int h = 0; h < V; h += 2) vld<S, 2>(p, idx + h, t + h);
+        } else {
+            vld<S, V>(p, idx, t);
+        }
+#pragma unroll
+        for (int q = 0; q < V; q++) o[q] = T(t[q]);
+    }
+}
+template <typename T, int V, typename S>
+__device__ __forceinline__ void vst_as(S *__restrict__ p, long long idx, const T *v)
+{
+    if constexpr (std::is_same<S, T>::value) {
+        vst<T, V>(p, idx, v);
+    } else {
+        S t[V];
+#pragma unroll
+        for (int q = 0; q < V; q++) t[q] = S(v[q]);
+        if constexpr (sizeof(S) == 8 && V % 2 == 0) {
+#pragma unroll
+            for (int h = 0; h < V; h += 2) vst<S, 2>(p, idx + h, t + h);
+        } else {
+            vst<S, V>(p, idx, t);
+        }
+    }
+}
+
 // Functor interface of the pass kernels.  A loader fills out[0..V-1] with the transform
 // input at (i, j, k+u), u < V (memory idx+u, consecutive along z); a storer consumes the
 // transform output for the same V elements.  A storer that reads state before writing it
 // (the spectral updates) exposes the read as pre() (PRE values per element into buf) and
 // the rest as fin(), so kernels can issue the reads of several elements before any write;
-// store() = pre() + fin().
-template <typename T>
+// store() = pre() + fin().  The pre() values have the storer's type Pre when it declares
+// one (pre_t), else the compute type.  LoadArr / StoreArr move an array of element type S.
+template <typename T, typename S = T>
 struct LoadArr {
-    const T *__restrict__ p;
+    const S *__restrict__ p;
     template <int V>
-    __device__ __forceinline__ void load(long long idx, int, int, int, T *out) const { vld<T, V>(p, idx, out); }
+    __device__ __forceinline__ void load(long long idx, int, int, int, T *out) const { vld_as<T, V, S>(p, idx, out); }
 };
-template <typename T>
+template <typename T, typename S = T>
 struct StoreArr {
-    T *__restrict__ p;
+    S *__restrict__ p;
     static constexpr int PRE = 0;
     template <int V>
     __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
     template <int V>
-    __device__ __forceinline__ void fin(long long idx, int, int, int, const T *v, const T *) const { vst<T, V>(p, idx, v); }
+    __device__ __forceinline__ void fin(long long idx, int, int, int, const T *v, const T *) const { vst_as<T, V, S>(p, idx, v); }
     template <int V>
-    __device__ __forceinline__ void store(long long idx, int, int, int, const T *v) const { vst<T, V>(p, idx, v); }
+    __device__ __forceinline__ void store(long long idx, int, int, int, const T *v) const { vst_as<T, V, S>(p, idx, v); }
 };
+
+template <class ST, typename T, class = void>
+struct pre_type { using type = T; };
+template <class ST, typename T>
+struct pre_type<ST, T, std::void_t<typename ST::Pre>> { using type = typename ST::Pre; };
+template <class ST, typename T>
+using pre_t = typename pre_type<ST, T>::type;
 
 // per-component kinds of the y and z transforms
 template <int NC>
@@ -224,9 +269,9 @@ __device__ __forceinline__ void pre_c(const ST &st, int comp, long long q, int i
     if constexpr (is_multi<ST>::value) st.template pre<V>(comp, q, i, j, k, buf);
     else st.template pre<V>(q, i, j, k, buf);
 }
-template <int V, class ST, typename T>
+template <int V, class ST, typename T, typename B>
 __device__ __forceinline__ void fin_c(const ST &st, int comp, long long q, int i, int j, int k, const T *v,
-                                      const T *buf)
+                                      const B *buf)
 {
     if constexpr (is_multi<ST>::value) st.template fin<V>(comp, q, i, j, k, v, buf);
     else st.template fin<V>(q, i, j, k, v, buf);

@@ -376,7 +376,8 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     // ---- stores: the storer's reads (pre) for a chunk of points go out before its writes
     constexpr int CH = 4;
     constexpr int PL = pre_len<ST, 2>();
-    auto put = [&](int pnt, bool edge, const T *pre_buf) {
+    using PB = pre_t<ST, T>;
+    auto put = [&](int pnt, bool edge, const PB *pre_buf) {
         const cpx<T> z = x1[pnt / R1][pnt % R1];
         const int o = out_row(pnt);
         const long long q = base + (long long)o * stride;
@@ -388,7 +389,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     if (full) {
 #pragma unroll
         for (int p0 = 0; p0 < NP; p0 += CH) {
-            T pre_buf[CH][PL];
+            PB pre_buf[CH][PL];
 #pragma unroll
             for (int u = 0; u < CH; u++) {
                 const int o = out_row(p0 + u);
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     } else {
 #pragma unroll
         for (int p0 = 0; p0 < NP; p0++) {
-            T pre_buf[PL];
+            PB pre_buf[PL];
             const int o = out_row(p0);
             if (nk >= 2) pre_c<2>(st, comp, base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
             put(p0, true, pre_buf);

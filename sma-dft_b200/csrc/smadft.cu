@@ -373,8 +373,9 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     }
     if (cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
     for (int s : slots_for(p->model)) {
-        if (cudaMalloc(&c.slot[s], c.esize * c.n) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
-        if (cudaMemset(c.slot[s], 0, c.esize * c.n) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+        const size_t bytes = (slot_is_state(s) ? sizeof(double) : c.esize) * c.n;
+        if (cudaMalloc(&c.slot[s], bytes) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
+        if (cudaMemset(c.slot[s], 0, bytes) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
     }
     for (int n : {p->nx, p->ny, p->nz}) {
         rc = c.f32 ? upload_plan<float>(c, n) : upload_plan<double>(c, n);
@@ -427,7 +428,8 @@ int smadft_set_psi(smadft_ctx *h, const double *host, size_t n)
     cudaSetDevice(c.dev);
     for (int s = 0; s < S_COUNT; s++)
         if (c.slot[s] && s != S_PSI) {
-            if (cudaMemsetAsync(c.slot[s], 0, c.esize * c.n, c.stream) != cudaSuccess)
+            if (cudaMemsetAsync(c.slot[s], 0, (slot_is_state(s) ? sizeof(double) : c.esize) * c.n, c.stream) !=
+                cudaSuccess)
                 return fail(c, SMADFT_ERR_CUDA, "memset");
         }
     int rc = c.f32 ? set_psi_t<float>(c, host) : set_psi_t<double>(c, host);
@@ -474,7 +476,7 @@ int smadft_get_field(smadft_ctx *h, int field, double *host, size_t n)
         rc = c.f32 ? ensure_psi<float>(c) : ensure_psi<double>(c);
         if (rc) return rc;
     }
-    return c.f32 ? get_slot_t<float>(c, slot, host) : get_slot_t<double>(c, slot, host);
+    return (c.f32 && !slot_is_state(slot)) ? get_slot_t<float>(c, slot, host) : get_slot_t<double>(c, slot, host);
 }
 
 // Runs one loop body by replaying its captured graph (captured on first use; the very

@@ -8,7 +8,9 @@ template <typename T>
 int adv_step(Ctx &c)
 {
     Spec<T> s = make_spec<T>(c);
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
+    T *psi = c.f<T>(S_PSI);
+    double *ph = c.f<double>(S_PSIH);   // spectral state (FP64)
+    T *np = c.f<T>(S_NP);
     T *gx = c.f<T>(S_GX), *gy = c.f<T>(S_GY), *gz = c.f<T>(S_GZ), *sp2 = c.f<T>(S_SP2);
     T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
     T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
@@ -19,8 +21,8 @@ int adv_step(Ctx &c)
         const int ky[5] = {K_DCT3, K_DCT3, K_DST3, K_DCT3, K_DCT3};
         const int kz[5] = {K_DCT3, K_DCT3, K_DCT3, K_DST3, K_DCT3};
         T *const out[5] = {psi, gx, gy, gz, sp2};
-        if ((rc = r2r3d_multi<T, 5>(c, kx, ky, kz, out, LoadArr<T>{ph}, LdGrad<T, 0>{s, ph}, LdGrad<T, 1>{s, ph},
-                                    LdGrad<T, 2>{s, ph}, LdNegLin<T>{s, ph})))
+        if ((rc = r2r3d_multi<T, 5>(c, kx, ky, kz, out, LoadArr<T, double>{ph}, LdGrad<T, 0, double>{s, ph},
+                                    LdGrad<T, 1, double>{s, ph}, LdGrad<T, 2, double>{s, ph}, LdNegLin<T>{s, ph})))
             return rc;
     }
     // force spectra S_c = ST_c(mu d_c psi) (:996-1027)

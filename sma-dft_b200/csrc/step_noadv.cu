@@ -9,32 +9,36 @@ template <typename T>
 int noadv_step(Ctx &c, bool keep_old)
 {
     Spec<T> s = make_spec<T>(c);
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
+    T *psi = c.f<T>(S_PSI);
+    double *ph = c.f<double>(S_PSIH);   // spectral state (FP64)
+    T *np = c.f<T>(S_NP);
     // N^n = REDFT10^3(beta psi^3 - gamma psi^5), fused CN/AB2 update of psihat
     int rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
                       StUpdCN<T>{make_spec<double>(c), ph, np});
     if (rc) return rc;
     // psi^{n+1} = REDFT01^3 psihat (into the second buffer when the old psi is needed)
     T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
-    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{ph}, StoreArr<T>{dst});
+    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T, double>{ph}, StoreArr<T>{dst});
 }
 
 template <typename T>
 int refresh_psi(Ctx &c, T *dst)
 {
-    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{c.f<T>(S_PSIH)}, StoreArr<T>{dst});
+    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T, double>{c.f<double>(S_PSIH)}, StoreArr<T>{dst});
 }
 
 template <typename T>
 int pre_loop(Ctx &c)
 {
     Spec<T> s = make_spec<T>(c);
-    T *psi = c.f<T>(S_PSI), *ph = c.f<T>(S_PSIH), *np = c.f<T>(S_NP);
+    T *psi = c.f<T>(S_PSI);
+    double *ph = c.f<double>(S_PSIH);
+    T *np = c.f<T>(S_NP);
     int rc;
     if (c.p.model == SMADFT_MODEL_QUASI) return quasi_pre_loop<T>(c);
     // psihat = scale REDFT10^3 psi ; Nprev = REDFT10^3(beta psi^3 - gamma psi^5) (no advection)
     // no-adv/cosNoAdvTrackSing.cpp:618-635, adv/cosAdvTrackMult.cpp:760-777
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, s.scale}))) return rc;
+    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, c.scale}))) return rc;
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma}, StoreArr<T>{np}))) return rc;
     return SMADFT_OK;
 }
@@ -43,14 +47,13 @@ template <typename T>
 int dfd_field(Ctx &c, T *dst)
 {
     Spec<T> s = make_spec<T>(c);
-    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdDfd<T>{s, c.f<T>(S_PSIH)}, StoreArr<T>{dst});
+    return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LdDfd<T>{s, c.f<double>(S_PSIH)}, StoreArr<T>{dst});
 }
 
 template <typename T>
 int psihat_from_psi(Ctx &c)
 {
-    Spec<T> s = make_spec<T>(c);
-    return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{c.f<T>(S_PSI)}, StScale<T>{c.f<T>(S_PSIH), s.scale});
+    return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{c.f<T>(S_PSI)}, StScale<T>{c.f<double>(S_PSIH), c.scale});
 }
 
 template <typename T>
