@@ -48,7 +48,7 @@ struct Spec {
     T eps, alpha, beta, gamma, q02, dtd2, dt, scale, nu;
     T rho_m, lam, kp, rho0;
     int nx, ny, nz;
-    long long nyz;
+    int nyz;
     __device__ __forceinline__ T mq2(int i, int j, int k) const
     {
         return qx[i] * qx[i] + qy[j] * qy[j] + qz[k] * qz[k];
@@ -235,8 +235,8 @@ template <typename T, int N>
 int launch_rdz(Ctx &c, int kind, const T *in, T *out)
 {
     const PlanDev &pd = c.plans.at(N);
-    const long long rows = (long long)c.g.nx * c.g.ny;
-    const long long tiles = (rows + 2 * kRdLines - 1) / (2 * kRdLines);
+    const int rows = c.g.nx * c.g.ny;
+    const int tiles = (rows + 2 * kRdLines - 1) / (2 * kRdLines);
     constexpr size_t smem = rdz_smem_bytes<T, N>();
     static bool attr_set = false;
     if (!attr_set) {

@@ -40,7 +40,7 @@ struct LdNonlin {
     const T *__restrict__ psi;
     T beta, gamma;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T p[V];
         vld<T, V>(psi, q, p);
@@ -57,11 +57,11 @@ struct LdGrad {
     Spec<T> s;
     const S *__restrict__ f;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         if (AX == 0 || AX == 1) {
             const bool in = AX == 0 ? (i < s.nx - 1) : (j < s.ny - 1);
-            const long long sh = AX == 0 ? s.nyz : (long long)s.nz;
+            const idx_t sh = AX == 0 ? s.nyz : (idx_t)s.nz;
             T v[V];
             vld_as<T, V, S>(f, in ? q + sh : q, v);
             const T sc = in ? -(AX == 0 ? s.sx[i] : s.sy[j]) : T(0);
@@ -84,7 +84,7 @@ struct LdNegLin {
     Spec<T> s;
     const double *__restrict__ ph;   // spectral state (FP64)
     template <int V>
-    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         T v[V];
         vld_as<T, V, double>(ph, q, v);
@@ -99,7 +99,7 @@ struct LdForce {
     const T *__restrict__ psi, *__restrict__ sp2, *__restrict__ g;
     T beta, gamma;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T a[V], b[V], c[V];
         vld<T, V>(psi, q, a);
@@ -124,12 +124,12 @@ struct LdStokes {
     // Branch-free: neighbours outside the box read a clamped in-range address and are
     // zeroed by selects; truncated modes are zeroed at the end.
     template <int V>
-    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         const T snu = s.scale / s.nu;
         if (AX == 0) {
             const bool live = i < s.nx - 1;
-            const long long qn = live ? q + s.nyz : q;         // (i+1, j, k)
+            const idx_t qn = live ? q + s.nyz : q;         // (i+1, j, k)
             const bool jy = j != 0;
             T sx[V], sy[V], d[V];
             vld<T, V>(Sx, q, sx);
@@ -152,7 +152,7 @@ struct LdStokes {
             }
         } else if (AX == 1) {
             const bool live = j < s.ny - 1;
-            const long long qj1 = live ? q + s.nz : q;          // (i, j+1, k)
+            const idx_t qj1 = live ? q + s.nz : q;          // (i, j+1, k)
             const bool ix = i != 0;
             T syv[V], sx[V], d[V];
             vld<T, V>(Sy, q, syv);
@@ -184,7 +184,7 @@ struct LdStokes {
             for (int u = 0; u < V; u++) {
                 const int kk = k + u;
                 const bool kl = kk < s.nz - 1;
-                const long long qk1 = kl ? q + 1 + u : q + u;    // (i, j, k+1)
+                const idx_t qk1 = kl ? q + 1 + u : q + u;    // (i, j, k+1)
                 const T sk = s.sz[kk];
                 const T sxr = Sx[ix ? qk1 - s.nyz : qk1];         // (i-1, j, k+1)
                 const T syr = Sy[jy ? qk1 - s.nz : qk1];          // (i, j-1, k+1)
@@ -206,7 +206,7 @@ struct LdAdvN {
     const T *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
     T beta, gamma;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T p[V], a[V], b[V], c[V], d[V], e[V], f[V];
         vld<T, V>(psi, q, p);
@@ -232,13 +232,13 @@ struct StUpdCN {
     static constexpr int PRE = 2;   // psihat, Nprev
     using Pre = double;
     template <int V>
-    __device__ __forceinline__ void pre(long long q, int, int, int, double *buf) const
+    __device__ __forceinline__ void pre(idx_t q, int, int, int, double *buf) const
     {
         vld<double, V>(ph, q, buf);
         vld_as<double, V, T>(np, q, buf + V);
     }
     template <int V>
-    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const double *buf) const
+    __device__ __forceinline__ void fin(idx_t q, int i, int j, int k, const T *v, const double *buf) const
     {
         double o[V];
 #pragma unroll
@@ -251,7 +251,7 @@ struct StUpdCN {
         vst<T, V>(np, q, v);
     }
     template <int V>
-    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    __device__ __forceinline__ void store(idx_t q, int i, int j, int k, const T *v) const
     {
         double buf[2 * V];
         pre<V>(q, i, j, k, buf);
@@ -266,14 +266,14 @@ struct StScale {
     double scale;
     static constexpr int PRE = 0;
     template <int V>
-    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    __device__ __forceinline__ void pre(idx_t, int, int, int, T *) const {}
     template <int V>
-    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *) const
+    __device__ __forceinline__ void fin(idx_t q, int i, int j, int k, const T *v, const T *) const
     {
         store<V>(q, i, j, k, v);
     }
     template <int V>
-    __device__ __forceinline__ void store(long long q, int, int, int, const T *v) const
+    __device__ __forceinline__ void store(idx_t q, int, int, int, const T *v) const
     {
         double o[V];
 #pragma unroll

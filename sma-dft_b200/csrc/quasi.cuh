@@ -15,7 +15,7 @@ struct LdDfd {
     Spec<T> s;
     const double *__restrict__ ph;   // spectral state (FP64)
     template <int V>
-    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         T v[V];
         vld_as<T, V, double>(ph, q, v);
@@ -30,7 +30,7 @@ struct LdLapDfd {
     Spec<T> s;
     const double *__restrict__ ph;   // spectral state (FP64)
     template <int V>
-    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         T v[V];
         vld_as<T, V, double>(ph, q, v);
@@ -48,7 +48,7 @@ struct LdRhoRaw {
     const T *__restrict__ psi, *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
     T kp, rho0, q02;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T p[V], a[V], b[V], c[V];
         vld<T, V>(psi, q, p); vld<T, V>(gx, q, a); vld<T, V>(gy, q, b); vld<T, V>(gz, q, c);
@@ -65,14 +65,14 @@ struct StFilter {
     T *__restrict__ out;
     static constexpr int PRE = 0;
     template <int V>
-    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    __device__ __forceinline__ void pre(idx_t, int, int, int, T *) const {}
     template <int V>
-    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *) const
+    __device__ __forceinline__ void fin(idx_t q, int i, int j, int k, const T *v, const T *) const
     {
         store<V>(q, i, j, k, v);
     }
     template <int V>
-    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    __device__ __forceinline__ void store(idx_t q, int i, int j, int k, const T *v) const
     {
         T o[V];
         const T exy = s.ex[i] * s.ey[j];
@@ -89,7 +89,7 @@ struct LdDivv {
     const T *__restrict__ rx, *__restrict__ ry, *__restrict__ rz;
     T dt;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T r[V], o[V], a[V], b[V], c[V], d[V], e[V], f[V];
         vld<T, V>(rho, q, r); vld<T, V>(ro, q, o);
@@ -106,7 +106,7 @@ template <typename T>
 struct LdMul {
     const T *__restrict__ a, *__restrict__ b;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T x[V], y[V];
         vld<T, V>(a, q, x);
@@ -123,14 +123,14 @@ struct StLapSpec {
     T *__restrict__ out;
     static constexpr int PRE = 0;
     template <int V>
-    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    __device__ __forceinline__ void pre(idx_t, int, int, int, T *) const {}
     template <int V>
-    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const T *) const
+    __device__ __forceinline__ void fin(idx_t q, int i, int j, int k, const T *v, const T *) const
     {
         store<V>(q, i, j, k, v);
     }
     template <int V>
-    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    __device__ __forceinline__ void store(idx_t q, int i, int j, int k, const T *v) const
     {
         T o[V];
 #pragma unroll
@@ -149,7 +149,7 @@ struct LdQForce {
     T eps, beta, gamma;
     int lap_rho;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T ps[V], f[V], lp[V], rh[V], gg[V], rr[V], mo[V], eo[V];
         vld<T, V>(psi, q, ps); vld<T, V>(dfd, q, f); vld<T, V>(lap, q, lp); vld<T, V>(rho, q, rh);
@@ -177,13 +177,13 @@ struct LdPressure {
     Spec<T> s;
     const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz, *__restrict__ dv;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         // branch-free: missing neighbours read a clamped address and are zeroed by selects
 #pragma unroll
         for (int u = 0; u < V; u++) {
             const int kk = k + u;
-            const long long qq = q + u;
+            const idx_t qq = q + u;
             const T sxr = Sx[i > 0 ? qq - s.nyz : qq];
             const T syr = Sy[j > 0 ? qq - s.nz : qq];
             const T szr = Sz[kk > 0 ? qq - 1 : qq];
@@ -208,7 +208,7 @@ struct LdQN {
     T kp;
     int extra;
     template <int V>
-    __device__ __forceinline__ void load(long long q, int, int, int, T *out) const
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
     {
         T m[V], a[V], b[V], c[V], d[V], e[V], f[V];
         vld<T, V>(mu, q, m);
@@ -239,14 +239,14 @@ struct StUpdBDF {
     static constexpr int PRE = 3;   // psihat, psihat_old, Nprev
     using Pre = double;
     template <int V>
-    __device__ __forceinline__ void pre(long long q, int, int, int, double *buf) const
+    __device__ __forceinline__ void pre(idx_t q, int, int, int, double *buf) const
     {
         vld<double, V>(ph, q, buf);
         vld<double, V>(pho, q, buf + V);
         vld_as<double, V, T>(np, q, buf + 2 * V);
     }
     template <int V>
-    __device__ __forceinline__ void fin(long long q, int i, int j, int k, const T *v, const double *buf) const
+    __device__ __forceinline__ void fin(idx_t q, int i, int j, int k, const T *v, const double *buf) const
     {
         double o[V];
 #pragma unroll
@@ -262,7 +262,7 @@ struct StUpdBDF {
         vst<T, V>(np, q, v);
     }
     template <int V>
-    __device__ __forceinline__ void store(long long q, int i, int j, int k, const T *v) const
+    __device__ __forceinline__ void store(idx_t q, int i, int j, int k, const T *v) const
     {
         double buf[3 * V];
         pre<V>(q, i, j, k, buf);

@@ -16,9 +16,13 @@
 
 namespace smadft {
 
+// Element index inside one field: grids are at most 1024 per axis, so every index
+// (< 1024^3 = 2^30) fits 32 bits, which keeps the per-element address arithmetic 32-bit.
+using idx_t = int;
+
 struct Geom {
     int nx, ny, nz;
-    long long nyz;   // ny * nz
+    int nyz;         // ny * nz
 };
 
 template <typename T>
@@ -70,7 +74,7 @@ __device__ __forceinline__ ElemPos elem_pos(const PassArgs<T> &a, int t, int w)
 // V consecutive elements p[idx .. idx+V-1]; for V > 1, idx is a multiple of V and p is
 // 16-byte aligned (one 8- or 16-byte access: float2 / float4 / double2).
 template <typename T, int V>
-__device__ __forceinline__ void vld(const T *__restrict__ p, long long idx, T *o)
+__device__ __forceinline__ void vld(const T *__restrict__ p, idx_t idx, T *o)
 {
     if constexpr (V == 4 && sizeof(T) == 4) {
         const float4 u = *reinterpret_cast<const float4 *>(p + idx);
@@ -88,7 +92,7 @@ __device__ __forceinline__ void vld(const T *__restrict__ p, long long idx, T *o
 }
 
 template <typename T, int V>
-__device__ __forceinline__ void vst(T *__restrict__ p, long long idx, const T *v)
+__device__ __forceinline__ void vst(T *__restrict__ p, idx_t idx, const T *v)
 {
     if constexpr (V == 4 && sizeof(T) == 4) {
         *reinterpret_cast<float4 *>(p + idx) = make_float4(v[0], v[1], v[2], v[3]);
@@ -105,7 +109,7 @@ __device__ __forceinline__ void vst(T *__restrict__ p, long long idx, const T *v
 // V elements of an array of element type S, converted to / from the compute type T (the
 // spectral state is FP64 for every compute precision); S == T is vld / vst.
 template <typename T, int V, typename S>
-__device__ __forceinline__ void vld_as(const S *__restrict__ p, long long idx, T *o)
+__device__ __forceinline__ void vld_as(const S *__restrict__ p, idx_t idx, T *o)
 {
     if constexpr (std::is_same<S, T>::value) {
         vld<T, V>(p, idx, o);
@@ -122,7 +126,7 @@ __device__ __forceinline__ void vld_as(const S *__restrict__ p, long long idx, T
     }
 }
 template <typename T, int V, typename S>
-__device__ __forceinline__ void vst_as(S *__restrict__ p, long long idx, const T *v)
+__device__ __forceinline__ void vst_as(S *__restrict__ p, idx_t idx, const T *v)
 {
     if constexpr (std::is_same<S, T>::value) {
         vst<T, V>(p, idx, v);
@@ -150,18 +154,18 @@ template <typename T, typename S = T>
 struct LoadArr {
     const S *__restrict__ p;
     template <int V>
-    __device__ __forceinline__ void load(long long idx, int, int, int, T *out) const { vld_as<T, V, S>(p, idx, out); }
+    __device__ __forceinline__ void load(idx_t idx, int, int, int, T *out) const { vld_as<T, V, S>(p, idx, out); }
 };
 template <typename T, typename S = T>
 struct StoreArr {
     S *__restrict__ p;
     static constexpr int PRE = 0;
     template <int V>
-    __device__ __forceinline__ void pre(long long, int, int, int, T *) const {}
+    __device__ __forceinline__ void pre(idx_t, int, int, int, T *) const {}
     template <int V>
-    __device__ __forceinline__ void fin(long long idx, int, int, int, const T *v, const T *) const { vst_as<T, V, S>(p, idx, v); }
+    __device__ __forceinline__ void fin(idx_t idx, int, int, int, const T *v, const T *) const { vst_as<T, V, S>(p, idx, v); }
     template <int V>
-    __device__ __forceinline__ void store(long long idx, int, int, int, const T *v) const { vst_as<T, V, S>(p, idx, v); }
+    __device__ __forceinline__ void store(idx_t idx, int, int, int, const T *v) const { vst_as<T, V, S>(p, idx, v); }
 };
 
 template <class ST, typename T, class = void>
@@ -192,7 +196,7 @@ struct LoadMulti<L0> {
     static constexpr bool MULTI = true;
     L0 h;
     template <int V, typename T>
-    __device__ __forceinline__ void load(int, long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(int, idx_t q, int i, int j, int k, T *out) const
     {
         h.template load<V>(q, i, j, k, out);
     }
@@ -206,7 +210,7 @@ struct LoadMulti<L0, L1, Ls...> {
     L0 h;
     LoadMulti<L1, Ls...> t;
     template <int V, typename T>
-    __device__ __forceinline__ void load(int comp, long long q, int i, int j, int k, T *out) const
+    __device__ __forceinline__ void load(int comp, idx_t q, int i, int j, int k, T *out) const
     {
         if (comp == 0) h.template load<V>(q, i, j, k, out);
         else t.template load<V>(comp - 1, q, i, j, k, out);
@@ -238,14 +242,14 @@ struct StoreMulti {
     T *p[NC];
     static constexpr int PRE = 0;
     template <int V>
-    __device__ __forceinline__ void pre(int, long long, int, int, int, T *) const {}
+    __device__ __forceinline__ void pre(int, idx_t, int, int, int, T *) const {}
     template <int V>
-    __device__ __forceinline__ void fin(int comp, long long idx, int, int, int, const T *v, const T *) const
+    __device__ __forceinline__ void fin(int comp, idx_t idx, int, int, int, const T *v, const T *) const
     {
         vst<T, V>(p[comp], idx, v);
     }
     template <int V>
-    __device__ __forceinline__ void store(int comp, long long idx, int, int, int, const T *v) const
+    __device__ __forceinline__ void store(int comp, idx_t idx, int, int, int, const T *v) const
     {
         vst<T, V>(p[comp], idx, v);
     }
@@ -258,26 +262,26 @@ struct KindSet {
 };
 
 template <int V, class LD, typename T>
-__device__ __forceinline__ void load_c(const LD &ld, int comp, long long q, int i, int j, int k, T *out)
+__device__ __forceinline__ void load_c(const LD &ld, int comp, idx_t q, int i, int j, int k, T *out)
 {
     if constexpr (is_multi<LD>::value) ld.template load<V>(comp, q, i, j, k, out);
     else ld.template load<V>(q, i, j, k, out);
 }
 template <int V, class ST, typename T>
-__device__ __forceinline__ void pre_c(const ST &st, int comp, long long q, int i, int j, int k, T *buf)
+__device__ __forceinline__ void pre_c(const ST &st, int comp, idx_t q, int i, int j, int k, T *buf)
 {
     if constexpr (is_multi<ST>::value) st.template pre<V>(comp, q, i, j, k, buf);
     else st.template pre<V>(q, i, j, k, buf);
 }
 template <int V, class ST, typename T, typename B>
-__device__ __forceinline__ void fin_c(const ST &st, int comp, long long q, int i, int j, int k, const T *v,
+__device__ __forceinline__ void fin_c(const ST &st, int comp, idx_t q, int i, int j, int k, const T *v,
                                       const B *buf)
 {
     if constexpr (is_multi<ST>::value) st.template fin<V>(comp, q, i, j, k, v, buf);
     else st.template fin<V>(q, i, j, k, v, buf);
 }
 template <int V, class ST, typename T>
-__device__ __forceinline__ void store_c(const ST &st, int comp, long long q, int i, int j, int k, const T *v)
+__device__ __forceinline__ void store_c(const ST &st, int comp, idx_t q, int i, int j, int k, const T *v)
 {
     if constexpr (is_multi<ST>::value) st.template store<V>(comp, q, i, j, k, v);
     else st.template store<V>(q, i, j, k, v);

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_plane_kernel(Geom g
     const int cid = blockIdx.x / PlaneInfo<N>::C;         // cluster
     const int i = cid / NC, comp = cid % NC;              // plane (x index), component
     const int kind_y = kinds.ky[comp], kind_z = kinds.kz[comp];
-    const long long pbase = (long long)i * g.nyz;         // element (i, 0, 0)
+    const idx_t pbase = i * g.nyz;                        // element (i, 0, 0)
     // thread (c, j) as in r2r_rd_kernel: c = complex line, j = first-stage butterfly
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5, hh16 = lane >> 4;
     const int c = lane & 15;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_plane_kernel(Geom g
                 const int t = e * NT + threadIdx.x;
                 const int ln = t / (N / 2), n = 2 * (t % (N / 2));
                 const int ja = r0 + 2 * ln;
-                const long long qa = pbase + (long long)ja * g.nz + n;
+                const idx_t qa = pbase + ja * g.nz + n;
                 l.template load<2>(qa, i, ja, n, va[e]);
                 l.template load<2>(qa + g.nz, i, ja + 1, n, vb[e]);
             }
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_plane_kernel(Geom g
         rd_fft<T, N>(v, x1, buf + c * RI::LD, wt, ht, j, wi, fwd, sine);
 
         // stores: the storer's reads (pre) for a chunk of points go out before its writes
-        const long long base = pbase + k;
+        const idx_t base = pbase + k;
         constexpr int CH = 4;
         constexpr int PL = pre_len<ST, 2>();
 #pragma unroll
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_plane_kernel(Geom g
 #pragma unroll
             for (int u = 0; u < CH; u++) {
                 const int o = rd_out_pos<N>(j, p0 + u, fwd, sine);
-                st.template pre<2>(comp, base + (long long)o * g.nz, i, o, k, pre_buf[u]);
+                st.template pre<2>(comp, base + o * g.nz, i, o, k, pre_buf[u]);
             }
 #pragma unroll
             for (int u = 0; u < CH; u++) {
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2) r2r_plane_kernel(Geom g
                 const cpx<T> z = x1[pnt / R1][pnt % R1];
                 const int o = rd_out_pos<N>(j, pnt, fwd, sine);
                 const T w2[2] = {z.x, z.y};
-                st.template fin<2>(comp, base + (long long)o * g.nz, i, o, k, w2, pre_buf[u]);
+                st.template fin<2>(comp, base + o * g.nz, i, o, k, w2, pre_buf[u]);
             }
         }
     }

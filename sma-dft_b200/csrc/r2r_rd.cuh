@@ -326,8 +326,8 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     const int kt = bt % tiles_b;
     const int a = bt / tiles_b;
     const int k = kt * 32 + 2 * c;                 // first of the two real lines
-    const long long stride = AXIS == 1 ? (long long)g.nz : g.nyz;
-    const long long base = (AXIS == 1 ? (long long)a * g.nyz : (long long)a * g.nz) + k;
+    const idx_t stride = AXIS == 1 ? g.nz : g.nyz;
+    const idx_t base = (AXIS == 1 ? a * g.nyz : a * g.nz) + k;
     const int nk = g.nz - k;                       // real lines of this pair inside the box
     const bool full = (kt + 1) * 32 <= g.nz;       // CTA-uniform: no line outside the box
     const bool fwd = (kind == K_DCT2 || kind == K_DST2);
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     // the pair of real samples (lines k, k+1) at line position t, packed as one complex;
     // the Loader computes them from its fields (each point is loaded exactly once)
     auto load_pair = [&](const auto &l, int t, bool edge) -> cpx<T> {
-        const long long q = base + (long long)t * stride;
+        const idx_t q = base + t * stride;
         const int ii = AXIS == 1 ? a : t, jj = AXIS == 1 ? t : a;
         T v[2] = {T(0), T(0)};
         if (!edge || nk >= 2) l.template load<2>(q, ii, jj, k, v);
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     auto put = [&](int pnt, bool edge, const PB *pre_buf) {
         const cpx<T> z = x1[pnt / R1][pnt % R1];
         const int o = out_row(pnt);
-        const long long q = base + (long long)o * stride;
+        const idx_t q = base + o * stride;
         const int ii = AXIS == 1 ? a : o, jj = AXIS == 1 ? o : a;
         const T w2[2] = {z.x, z.y};
         if (!edge || nk >= 2) fin_c<2>(st, comp, q, ii, jj, k, w2, pre_buf);
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
 #pragma unroll
             for (int u = 0; u < CH; u++) {
                 const int o = out_row(p0 + u);
-                pre_c<2>(st, comp, base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
+                pre_c<2>(st, comp, base + o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
             }
 #pragma unroll
             for (int u = 0; u < CH; u++) put(p0 + u, false, pre_buf[u]);
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
         for (int p0 = 0; p0 < NP; p0++) {
             PB pre_buf[PL];
             const int o = out_row(p0);
-            if (nk >= 2) pre_c<2>(st, comp, base + (long long)o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
+            if (nk >= 2) pre_c<2>(st, comp, base + o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
             put(p0, true, pre_buf);
         }
     }

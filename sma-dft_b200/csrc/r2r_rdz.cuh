@@ -24,7 +24,7 @@ constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * s
 
 // rows = number of z lines (nx * ny); a CTA transforms 2 * kRdLines consecutive rows
 template <typename T, int N>
-__global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(long long rows, int kind, const T *in, T *out,
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind, const T *in, T *out,
                                                                         const cpx<T> *__restrict__ wt_g,
                                                                         const cpx<T> *__restrict__ ht_g)
 {
@@ -44,9 +44,9 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     }
     const int j = threadIdx.x % R1;                 // first-stage butterfly (lane in its group)
     const int c = threadIdx.x / R1;                 // complex line of the CTA
-    const long long ra = (long long)blockIdx.x * (2 * kRdLines) + 2 * c;   // real rows ra, ra + 1
+    const int ra = (int)blockIdx.x * (2 * kRdLines) + 2 * c;   // real rows ra, ra + 1
     const bool oka = ra < rows, okb = ra + 1 < rows;
-    const long long ia = (oka ? ra : 0) * N, ib = (okb ? ra + 1 : 0) * N;
+    const idx_t ia = (oka ? ra : 0) * N, ib = (okb ? ra + 1 : 0) * N;
     const bool fwd = (kind == K_DCT2 || kind == K_DST2);
     const bool sine = (kind == K_DST2 || kind == K_DST3);
 

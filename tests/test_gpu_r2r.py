@@ -55,11 +55,13 @@ def test_plane_kernel_matches_separate_passes(shape, precision, monkeypatch):
     assert np.max(np.abs(got["1"] - got["0"])) <= tol * np.max(np.abs(got["0"]))
 
 
-@pytest.mark.parametrize("shape", [(8, 8, 64), (6, 10, 128), (4, 16, 256)], ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("shape", [(8, 8, 64), (6, 10, 128), (4, 16, 256), (60, 250, 256)],
+                         ids=lambda s: "x".join(map(str, s)))
 @pytest.mark.parametrize("precision", [smadft.FP64, smadft.FP32], ids=["fp64", "fp32"])
 @pytest.mark.parametrize("kinds", [(0, 0, 0), (1, 1, 1), (2, 2, 2), (3, 3, 3)], ids=lambda k: "".join(map(str, k)))
 def test_rdz_kernel_matches_staged_z(shape, precision, kinds, monkeypatch):
-    """Register-direct z kernel against the staged z kernel (SMADFT_RDZ=0), all four kinds."""
+    """Register-direct z kernel against the staged z kernel (SMADFT_RDZ=0), all four kinds,
+    partial last tiles included."""
     x = np.random.default_rng(23).standard_normal(shape)
     got = {}
     for flag in ("1", "0"):
