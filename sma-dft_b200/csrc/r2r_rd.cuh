@@ -293,6 +293,37 @@ __device__ __forceinline__ int rd_out_pos(int j, int pnt, bool fwd, bool sine)
     return kk < N / 2 ? 2 * kk : 2 * (N - 1 - kk) + 1;
 }
 
+// Line positions of butterfly j as affine maps of the (compile-time) point index.  The
+// natural position read by stage-0 point q is lb + ls q when q R1 < N/2, else hb + hs q;
+// the position of output point pnt is olb + ols C, else ohb + ohs C, with
+// C = (pnt / R1) R1 + R0 (pnt mod R1) against N/2 (j < R1 never moves a point across N/2,
+// which is a multiple of R0 and R1).  Inside the unrolled loops the branch folds and one
+// multiply-add per point remains (the maps equal makhoul_src / rd_out_pos).
+template <int N>
+struct RdPos {
+    static constexpr int R0 = RdInfo<N>::R0, R1 = RdInfo<N>::R1;
+    int lb, ls, hb, hs, olb, ols, ohb, ohs;
+    __device__ __forceinline__ RdPos(int j, bool fwd, bool sine)
+    {
+        if (fwd) {
+            lb = 2 * j; ls = 2 * R1; hb = 2 * N - 1 - 2 * j; hs = -2 * R1;   // Makhoul order
+            olb = ohb = sine ? N - 1 - j : j;
+            ols = ohs = sine ? -1 : 1;
+        } else {
+            lb = hb = sine ? N - 1 - j : j;
+            ls = hs = sine ? -R1 : R1;
+            olb = 2 * j; ols = 2; ohb = 2 * N - 1 - 2 * j; ohs = -2;         // y[2m], y[2m+1]
+        }
+    }
+    static constexpr bool src_lo(int q) { return q * R1 < N / 2; }
+    static constexpr int cpos(int pnt) { return (pnt / R1) * R1 + R0 * (pnt % R1); }
+    __device__ __forceinline__ int src(int q) const { return src_lo(q) ? lb + ls * q : hb + hs * q; }
+    __device__ __forceinline__ int out(int pnt) const
+    {
+        return cpos(pnt) < N / 2 ? olb + ols * cpos(pnt) : ohb + ohs * cpos(pnt);
+    }
+};
+
 // NC > 1: multi-component pass (LoadMulti / StoreMulti); CTA b transforms component b mod NC
 // of tile b / NC, so the components' shared input reads meet in L2.
 template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
@@ -334,20 +365,29 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     const bool sine = (kind == K_DST2 || kind == K_DST3);
     __syncthreads();
 
-    // the pair of real samples (lines k, k+1) at line position t, packed as one complex;
+    // element indices: position t of a line point sits at base + t * stride, so the affine
+    // position maps become affine index maps (one multiply-add per point)
+    const RdPos<N> pos(j, fwd, sine);
+    const idx_t slo = base + pos.lb * stride, dslo = pos.ls * stride;
+    const idx_t shi = base + pos.hb * stride, dshi = pos.hs * stride;
+    const idx_t olo = base + pos.olb * stride, dolo = pos.ols * stride;
+    const idx_t ohi = base + pos.ohb * stride, dohi = pos.ohs * stride;
+    auto src_idx = [&](int q) -> idx_t { return RdPos<N>::src_lo(q) ? slo + q * dslo : shi + q * dshi; };
+    auto out_idx = [&](int pnt) -> idx_t {
+        constexpr int H = N / 2;
+        const int C = RdPos<N>::cpos(pnt);
+        return C < H ? olo + C * dolo : ohi + C * dohi;
+    };
+
+    // the pair of real samples (lines k, k+1) of stage-0 point q, packed as one complex;
     // the Loader computes them from its fields (each point is loaded exactly once)
-    auto load_pair = [&](const auto &l, int t, bool edge) -> cpx<T> {
-        const idx_t q = base + t * stride;
+    auto load_pair = [&](const auto &l, int q, bool edge) -> cpx<T> {
+        const int t = pos.src(q);
         const int ii = AXIS == 1 ? a : t, jj = AXIS == 1 ? t : a;
         T v[2] = {T(0), T(0)};
-        if (!edge || nk >= 2) l.template load<2>(q, ii, jj, k, v);
-        else if (nk == 1) l.template load<1>(q, ii, jj, k, v);
+        if (!edge || nk >= 2) l.template load<2>(src_idx(q), ii, jj, k, v);
+        else if (nk == 1) l.template load<1>(src_idx(q), ii, jj, k, v);
         return {v[0], v[1]};
-    };
-    auto src_pos = [&](int q) -> int {       // natural line position of stage-0 point q
-        const int p = j + q * R1;
-        if (fwd) return makhoul_src<N>(p);
-        return sine ? N - 1 - p : p;
     };
 
     cpx<T> v[R0];
@@ -355,23 +395,24 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     visit_c(ld, comp, [&](const auto &l) {
         if (full) {
 #pragma unroll
-            for (int q = 0; q < R0; q++) v[q] = load_pair(l, src_pos(q), false);
+            for (int q = 0; q < R0; q++) v[q] = load_pair(l, q, false);
         } else {
 #pragma unroll
-            for (int q = 0; q < R0; q++) v[q] = load_pair(l, src_pos(q), true);
+            for (int q = 0; q < R0; q++) v[q] = load_pair(l, q, true);
         }
     });
     if (fwd) {
-        // Makhoul-permuted input: DST-II negates odd natural samples
+        // Makhoul-permuted input: DST-II negates odd natural samples (the odd ones are the
+        // upper half, q R1 >= N/2)
         if (sine) {
 #pragma unroll
             for (int q = 0; q < R0; q++)
-                if (src_pos(q) & 1) v[q] = {-v[q].x, -v[q].y};
+                if (!RdPos<N>::src_lo(q)) v[q] = {-v[q].x, -v[q].y};
         }
     }
     cpx<T> x1[BPT][R1];
     rd_fft<T, N>(v, x1, buf + c * RI::LD, wt, ht, j, wi, fwd, sine);
-    auto out_row = [&](int pnt) -> int { return rd_out_pos<N>(j, pnt, fwd, sine); };
+    auto out_row = [&](int pnt) -> int { return pos.out(pnt); };
 
     // ---- stores: the storer's reads (pre) for a chunk of points go out before its writes
     constexpr int CH = 4;
@@ -380,7 +421,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
     auto put = [&](int pnt, bool edge, const PB *pre_buf) {
         const cpx<T> z = x1[pnt / R1][pnt % R1];
         const int o = out_row(pnt);
-        const idx_t q = base + o * stride;
+        const idx_t q = out_idx(pnt);
         const int ii = AXIS == 1 ? a : o, jj = AXIS == 1 ? o : a;
         const T w2[2] = {z.x, z.y};
         if (!edge || nk >= 2) fin_c<2>(st, comp, q, ii, jj, k, w2, pre_buf);
@@ -393,7 +434,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
 #pragma unroll
             for (int u = 0; u < CH; u++) {
                 const int o = out_row(p0 + u);
-                pre_c<2>(st, comp, base + o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
+                pre_c<2>(st, comp, out_idx(p0 + u), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
             }
 #pragma unroll
             for (int u = 0; u < CH; u++) put(p0 + u, false, pre_buf[u]);
@@ -403,7 +444,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2
         for (int p0 = 0; p0 < NP; p0++) {
             PB pre_buf[PL];
             const int o = out_row(p0);
-            if (nk >= 2) pre_c<2>(st, comp, base + o * stride, AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
+            if (nk >= 2) pre_c<2>(st, comp, out_idx(p0), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
             put(p0, true, pre_buf);
         }
     }

@@ -50,15 +50,16 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     const bool fwd = (kind == K_DCT2 || kind == K_DST2);
     const bool sine = (kind == K_DST2 || kind == K_DST3);
 
+    const RdPos<N> pos(j, fwd, sine);               // affine position maps (r2r_rd.cuh)
+    const T *pa = in + ia, *pb = in + ib;
     cpx<T> v[R0];
 #pragma unroll
     for (int q = 0; q < R0; q++) {
-        const int p = j + q * R1;
-        const int n = fwd ? makhoul_src<N>(p) : (sine ? N - 1 - p : p);
-        T a = in[ia + n], b = in[ib + n];
+        const int n = pos.src(q);
+        T a = pa[n], b = pb[n];
         if (!oka) a = T(0);
         if (!okb) b = T(0);
-        if (fwd && sine && (n & 1)) {                // DST-II negates odd natural samples
+        if (fwd && sine && !RdPos<N>::src_lo(q)) {   // DST-II negates odd natural samples
             a = -a;
             b = -b;
         }
@@ -67,12 +68,13 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     __syncthreads();                                 // twiddle tables
     cpx<T> x1[BPT][R1];
     rd_fft<T, N, true>(v, x1, buf + c * RI::LD, wt, ht, j, threadIdx.x >> 5, fwd, sine, wz);
+    T *qa = out + ia, *qb = out + ib;
 #pragma unroll
     for (int pnt = 0; pnt < NP; pnt++) {
         const cpx<T> z = x1[pnt / R1][pnt % R1];
-        const int o = rd_out_pos<N>(j, pnt, fwd, sine);
-        if (oka) out[ia + o] = z.x;
-        if (okb) out[ib + o] = z.y;
+        const int o = pos.out(pnt);
+        if (oka) qa[o] = z.x;
+        if (okb) qb[o] = z.y;
     }
 }
 
