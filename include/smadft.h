@@ -193,6 +193,37 @@ int smadft_r2r3d_device(smadft_ctx *ctx, const void *in, void *out, int kx, int 
 int smadft_r2r3d_noalloc(const void *in, void *out, int nx, int ny, int nz, int kx, int ky, int kz,
                          int precision, void *stream);
 
+/* ---- batches: independent runs advanced by one captured step ---------------------------
+ * The batched parameter sweep of the north star (many runs of uneven grids and parameters):
+ * the reference runs each as its own MPI job.  A batch owns n contexts (any model, grid,
+ * precision and parameters; one device); smadft_batch_step advances every member by nsteps
+ * loop bodies, each body one CUDA graph that runs all members' kernels concurrently.
+ * Members are ordinary contexts for everything else (smadft_batch_member): set their
+ * initial conditions, read fields, track, checkpoint.  A batch is not thread-safe. */
+typedef struct smadft_batch smadft_batch;
+int smadft_batch_create(const smadft_params *params, int n, smadft_batch **out);
+int smadft_batch_destroy(smadft_batch *batch);
+int smadft_batch_size(const smadft_batch *batch, int *n);
+int smadft_batch_member(smadft_batch *batch, int i, smadft_ctx **ctx);
+int smadft_batch_step(smadft_batch *batch, int nsteps);
+int smadft_batch_sync(smadft_batch *batch);
+const char *smadft_batch_last_error(const smadft_batch *batch);
+
+/* ---- kernel-path autotuner ---------------------------------------------------------------
+ * Times `steps` loop bodies of each applicable kernel-path configuration on this context
+ * (register-direct or staged passes, fused plane kernel, grouped y passes, forked chains)
+ * and keeps the fastest; the run's state is restored after every trial, so stepping
+ * continues exactly as without the call.  ms[i] = time per body of configuration i (-1:
+ * not applicable to this grid), named by smadft_tune_config_name(i).  Synchronises. */
+#define SMADFT_TUNE_MAX 8
+typedef struct {
+    int configs;                  /* configurations timed                    */
+    int chosen;                   /* index of the one kept                   */
+    double ms[SMADFT_TUNE_MAX];   /* milliseconds per loop body, -1 = skipped */
+} smadft_tune_report;
+int smadft_autotune(smadft_ctx *ctx, int steps, smadft_tune_report *out);
+const char *smadft_tune_config_name(int i);
+
 /* ---- initial-condition builders (host only, no device) --------------------------------
  * All write nx*ny*nz doubles in the reference layout; grid spacing dx = 2 pi/(q0 nw). */
 /* Flat x-normal interface: A cos(q0 z) 1/2 (1 - tanh((x - x0)/(2 lambda0))) + U(+-noise),

@@ -614,3 +614,4 @@ int smadft_r2r3d_device(smadft_ctx *h, const void *in, void *out, int kx, int ky
 }  // extern "C"
 
 #include "checkpoint.inc"
+#include "batch.inc"

@@ -61,6 +61,11 @@ class Diag(ctypes.Structure):
                     steps=int(self.steps), nonfinite=int(self.nonfinite))
 
 
+class TuneReport(ctypes.Structure):
+    """smadft_tune_report"""
+    _fields_ = [("configs", ctypes.c_int), ("chosen", ctypes.c_int), ("ms", ctypes.c_double * 8)]
+
+
 # (name, restype, argtypes) of every exported entry point declared in include/smadft.h
 _P = ctypes.POINTER
 _dp = _P(ctypes.c_double)
@@ -91,6 +96,15 @@ SIGNATURES = [
     ("smadft_launch_count", ctypes.c_int, [_vp, _P(ctypes.c_longlong)]),
     ("smadft_r2r3d_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    ("smadft_batch_create", ctypes.c_int, [_P(Params), ctypes.c_int, _P(_vp)]),
+    ("smadft_batch_destroy", ctypes.c_int, [_vp]),
+    ("smadft_batch_size", ctypes.c_int, [_vp, _P(ctypes.c_int)]),
+    ("smadft_batch_member", ctypes.c_int, [_vp, ctypes.c_int, _P(_vp)]),
+    ("smadft_batch_step", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("smadft_batch_sync", ctypes.c_int, [_vp]),
+    ("smadft_batch_last_error", ctypes.c_char_p, [_vp]),
+    ("smadft_autotune", ctypes.c_int, [_vp, ctypes.c_int, _P(TuneReport)]),
+    ("smadft_tune_config_name", ctypes.c_char_p, [ctypes.c_int]),
     ("smadft_ic_interface", ctypes.c_int, [_P(Params), ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_ulonglong, _dp]),
     ("smadft_ic_focal_conic", ctypes.c_int, [_P(Params), ctypes.c_double, ctypes.c_double, _dp]),
@@ -270,6 +284,69 @@ class Solver:
         _check(lib().smadft_r2r_pass_device(self._h, _vp(src_ptr), _vp(dst_ptr), int(axis), int(kind)),
                self._h)
 
+    def autotune(self, steps: int = 5) -> dict:
+        """Time each applicable kernel path on this run and keep the fastest (state kept)."""
+        r = TuneReport()
+        _check(lib().smadft_autotune(self._h, int(steps), ctypes.byref(r)), self._h)
+        ms = {lib().smadft_tune_config_name(i).decode(): r.ms[i] for i in range(8) if r.ms[i] > 0}
+        return {"chosen": lib().smadft_tune_config_name(r.chosen).decode(), "ms_per_step": ms}
+
     def r2r3d_device(self, src_ptr: int, dst_ptr: int, kinds) -> None:
         _check(lib().smadft_r2r3d_device(self._h, _vp(src_ptr), _vp(dst_ptr), *[int(k) for k in kinds]),
                self._h)
+
+
+class _Member(Solver):
+    """A batch member: a context owned by its batch (closing it is a no-op)."""
+
+    def __init__(self, handle, p: Params):
+        self.p = p
+        self.shape = (p.nx, p.ny, p.nz)
+        self.n = p.nx * p.ny * p.nz
+        self._h = handle
+
+    def close(self):
+        self._h = None
+
+
+class Batch:
+    """Independent runs advanced together (``smadft_batch``): one CUDA graph per step for all."""
+
+    def __init__(self, plist):
+        arr = (Params * len(plist))(*plist)
+        h = _vp()
+        _check(lib().smadft_batch_create(arr, len(plist), ctypes.byref(h)))
+        self._h = h
+        self.members = []
+        for i, p in enumerate(plist):
+            m = _vp()
+            _check(lib().smadft_batch_member(h, i, ctypes.byref(m)))
+            self.members.append(_Member(m, p))
+
+    def step(self, n: int = 1) -> None:
+        rc = lib().smadft_batch_step(self._h, int(n))
+        if rc:
+            raise SmadftError(rc, lib().smadft_batch_last_error(self._h).decode())
+
+    def sync(self) -> None:
+        _check(lib().smadft_batch_sync(self._h))
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            for m in self.members:
+                m._h = None
+            lib().smadft_batch_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

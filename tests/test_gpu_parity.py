@@ -238,3 +238,26 @@ def test_step_before_psi_is_state_error():
         with pytest.raises(smadft.SmadftError) as e:
             s.step(1)
         assert e.value.code == -8
+
+
+def test_config2_noadv_256_fp32_interface_error():
+    """Config 2: noadv 256^3, bump interface x0(y) = L/2 + 2 lambda0 sin(2 pi y / Ly), dt 0.05,
+    10^4 steps, FP32 fields against the FP64 path: interface position (bump tracker along x,
+    FP64 sub-grid crossing) within 0.01 lambda0, relative L2 of psi below 2e-5 (measured
+    1.4e-5; the smectic half melts at eps = -0.75, so psi's norm falls to a third)."""
+    shape = (256, 256, 256)
+    p = smadft.params(smadft.NOADV, shape, dt=0.05)
+    psi0 = smadft.ic_interface(p, A=1.328, bump=2 * 2 * np.pi, noise=1e-3, seed=20240601)
+    out = {}
+    for prec in (smadft.FP32, smadft.FP64):
+        with smadft.Solver(smadft.params(smadft.NOADV, shape, dt=0.05, precision=prec)) as s:
+            s.set_psi(psi0)
+            s.step(10000)
+            out[prec] = (s.get("psi"), s.track(axis=0, mode=smadft.TRACK_BUMP, hi=0.6, lo=0.1))
+    (a, (ia, pa)), (b, (ib, pb)) = out[smadft.FP32], out[smadft.FP64]
+    assert np.all(np.isfinite(a)) and np.all(np.isfinite(b))
+    assert rel_l2(a, b) <= 2e-5
+    found = np.isfinite(pa) & np.isfinite(pb)
+    assert found.sum() > 0.5 * found.size
+    lam0_cells = p.nw                      # lambda0 = nw grid cells
+    assert np.max(np.abs(pa[found] - pb[found])) / lam0_cells <= 0.01
