@@ -244,6 +244,86 @@ def pass_roofline(torch, smadft, peak):
         return out
 
 
+def sweep_params(smadft):
+    """Config 4: 48 runs, 12 each of 64^3 / 96^3 / 128^3 / 160^3, noadv and adv alternating,
+    eps ~ U[-0.85, -0.65], gamma in {0.8, 1.0, 1.2}, FP32 fields (FP64 state and reductions),
+    seeded per run (seed 20240601 + run)."""
+    rng = np.random.default_rng(20240601)
+    runs = []
+    for r in range(48):
+        n = (64, 96, 128, 160)[r % 4]
+        model = smadft.NOADV if (r // 4) % 2 == 0 else smadft.ADV
+        kw = dict(eps=float(rng.uniform(-0.85, -0.65)), gamma=(0.8, 1.0, 1.2)[r % 3],
+                  dt=0.05 if model == smadft.NOADV else 0.01)
+        runs.append((model, n, kw, 20240601 + r))
+    return runs
+
+
+def run_batch_sweep(torch, smadft, steps, rank, world, dist):
+    """Config 4 through smadft_batch: this rank's share of the 48 runs (greedy by cost
+    N^3 F, F = 6 noadv / 32 adv), each autotuned, then `steps` batch steps timed with CUDA
+    events on the batch; the same runs stepped one context after another for comparison."""
+    runs = sweep_params(smadft)
+    load = [0.0] * world
+    mine = []
+    for idx in sorted(range(len(runs)), key=lambda i: -runs[i][1] ** 3 * (6 if runs[i][0] == smadft.NOADV else 32)):
+        r = min(range(world), key=lambda w: load[w])
+        load[r] += runs[idx][1] ** 3 * (6 if runs[idx][0] == smadft.NOADV else 32)
+        if r == rank:
+            mine.append(idx)
+    plist = []
+    for i in sorted(mine):
+        model, n, kw, _ = runs[i]
+        plist.append(smadft.params(model, (n, n, n), precision=smadft.FP32, **kw))
+    ics = []
+    for (i, p) in zip(sorted(mine), plist):
+        seed = runs[i][3]
+        if p.model == smadft.NOADV:
+            ics.append(smadft.ic_interface(p, A=1.328, bump=0.0, noise=1e-3, seed=seed))
+        else:
+            ics.append(smadft.ic_conics(p, A=1.328, count=4, rmin=1.0, rmax=2.0, noise=1e-3, seed=seed))
+    out = {}
+    with smadft.Batch(plist) as b:
+        for m, psi in zip(b.members, ics):
+            m.set_psi(psi)
+        tuned = {}
+        for m in b.members:
+            rep = m.autotune(2)
+            tuned[rep["chosen"]] = tuned.get(rep["chosen"], 0) + 1
+        b.step(3)
+        b.sync()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.step(steps)
+        b.sync()
+        ms_batch = 1000.0 * (time.perf_counter() - t0)
+        finite = all(bool(np.all(np.isfinite(m.get("psi")))) for m in b.members)
+        # the same members stepped one after another (each on its own graph)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for m in b.members:
+            m.step(steps)
+        for m in b.members:
+            m.sync()
+        ms_solo = 1000.0 * (time.perf_counter() - t0)
+    if world > 1:
+        t = torch.tensor([ms_batch, ms_solo], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_batch, ms_solo = float(t[0]), float(t[1])
+        c = torch.tensor([float(finite)], device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.MIN)
+        finite = bool(c.item())
+    total = len(runs) * steps
+    out = {"runs": len(runs), "runs_on_rank0": len(plist), "steps": steps,
+           "grids": "12 each of 64^3, 96^3, 128^3, 160^3; noadv/adv alternating; FP32",
+           "aggregate_steps_per_s": total / (ms_batch / 1000.0),
+           "ms_per_batch_step": ms_batch / steps,
+           "sequential_aggregate_steps_per_s": total / (ms_solo / 1000.0),
+           "autotuned_paths_rank0": tuned, "finite": finite,
+           "timing": "host wall clock around batch_step + sync, max over ranks"}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import smadft
@@ -261,10 +341,12 @@ def run_ours(args, rank, world, local_rank):
     launches_fp32 = 0
     clocks = {}
     solvers = {}
+    tuned = {}
     for prec, name in ((smadft.FP32, "fp32"), (smadft.FP64, "fp64")):
         p = smadft.params(smadft.ADV, (N, N, N), precision=prec, device=local_rank, **CFG)
         s = solvers[name] = smadft.Solver(p)
         s.set_psi(psi0)
+        tuned[name] = s.autotune(3)["chosen"]      # kernel path per grid and precision
         s.step(args.warmup)
         s.sync()
         if name == "fp32":
@@ -321,6 +403,7 @@ def run_ours(args, rank, world, local_rank):
             e2e_ms = float(t.item())
     e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
 
+    sweep = run_batch_sweep(torch, smadft, args.sweep_steps, rank, world, dist) if args.sweep_steps > 0 else None
     passes = pass_roofline(torch, smadft, peak) if rank == 0 else {}
     if world > 1:
         dist.barrier()
@@ -352,6 +435,7 @@ def run_ours(args, rank, world, local_rank):
         "err_after_steps": err_steps,
         "rel_l2_err_after_timed_steps": err_timed,
         "state_precision": "psihat (the spectral state) in FP64, time update in FP64",
+        "autotuned_path": tuned,
         "roofline": {"bound": "hbm", "achieved": zp.get("gbs"), "peak": peak, "unit": "GB/s",
                      "frac": zp.get("frac"), "traffic": profile_traffic("r2r_rdz_z_pass_256cube_fp32.md"),
                      "peak_source": f"{peak_kind} hbm_gbs",
@@ -365,6 +449,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 8 * N ** 3,
                 "d2h_bytes_per_step": 8 * N ** 3},
         "gpu_launches": launches_fp32,
+        "batch_sweep": sweep,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
@@ -414,6 +499,8 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--sweep-steps", type=int, default=200,
+                    help="steps of the 48-run batched sweep (config 4 runs 2000; 0: skip)")
     ap.add_argument("--err-steps", type=int, default=ERR_STEPS,
                     help="steps after which the FP32 error against FP64 is reported (0: after the timed steps)")
     ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "r2r3d", "step"], default=None,
