@@ -70,6 +70,7 @@ def lib():
         L.orc_track.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.c_double, ctypes.c_double,
                                 ctypes.POINTER(ctypes.c_int), dp]
+        L.orc_step_surface.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), dp, dp, dp]
         L.orc_r2r_1d.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int]
         L.orc_r2r_3d.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                  ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -158,6 +159,18 @@ class Oracle:
         lib().orc_track(self._c, field, axis, mode, hi, lo,
                         idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(pos))
         return idx, pos
+
+    def step_surface(self):
+        """One step with the surface diagnostics: per (i, j) column the interface index
+        along z (-1: none), normal velocity, 2H and K (NaN: none)."""
+        shp = (self.shape[0], self.shape[1])
+        idx = np.empty(shp, dtype=np.int32)
+        vel, h, k = (np.empty(shp) for _ in range(3))
+        rc = lib().orc_step_surface(self._c, idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(vel), _dp(h),
+                                    _dp(k))
+        if rc:
+            raise RuntimeError("orc_step_surface failed")
+        return idx, vel, h, k
 
 
 # ----------------------------------------------------------------------------------

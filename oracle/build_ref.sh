@@ -11,7 +11,7 @@
 #   * the IC block is kept; refshim_load_ic() may overwrite psi afterwards (REFSHIM_IC)
 #   * output directories                              -> REFSHIM_DIR
 #   * psiMid's hard-coded j = 256 (noadv Sing)        -> Ny/2 (in range for small grids)
-#   * L1/mass/energy text output                      -> 17 significant digits
+#   * L1/mass/energy/velSurf/curvH/curvK text output  -> 17 significant digits
 #   * before MPI::Finalize(), binary dumps of the final fields
 # Usage: oracle/build_ref.sh   (writes oracle/_ref/{noadv,bump,adv,quasi}_ref)
 set -euo pipefail
@@ -38,6 +38,9 @@ COMMON=(
   -e "s/const double alpha =  \([0-9.]*\);/const double alpha = $P(\"ALPHA\", \1);/"
   -e "s/while (L1 > limL1)/for (long refshim_s = 0; refshim_s < refshim_steps(); refshim_s++)/"
   -e "s/L1_output << L1 << /L1_output << std::setprecision(17) << L1 << /"
+  -e "s/velS_output << velSurf\[index\] << /velS_output << std::setprecision(17) << velSurf[index] << /"
+  -e "s/curvH_output << curvH\[index\] << /curvH_output << std::setprecision(17) << curvH[index] << /"
+  -e "s/curvK_output << curvK\[index\] << /curvK_output << std::setprecision(17) << curvK[index] << /"
 )
 
 build() { # name source extra-sed-args... ; dump statement is passed in DUMP

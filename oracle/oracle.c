@@ -31,6 +31,11 @@ struct orc_ctx {
     /* quasi */
     double *psiq_old, *psi_old, *rho, *rhoq, *rho_old, *p_, *divv, *mu, *energy, *dfd, *lap;
     double *rdx, *rdy, *rdz;
+    /* surface diagnostics of one step (orc_step_surface) */
+    int surf_pending;
+    double *dTpsi, *psiDxx, *psiDyy, *psiDzz, *fgx, *fgy, *fgz;
+    int *s_idx;
+    double *s_vel, *s_H, *s_K;
     long nloop;
     double L1, mass, en;
     int have_psi;
@@ -137,6 +142,8 @@ void orc_destroy(orc_ctx *c)
                        &c->psiq_old, &c->psi_old, &c->rho, &c->rhoq, &c->rho_old, &c->p_,
                        &c->divv, &c->mu, &c->energy, &c->dfd, &c->lap, &c->rdx, &c->rdy, &c->rdz};
     for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); q++) free(*ptrs[q]);
+    free(c->dTpsi); free(c->psiDxx); free(c->psiDyy); free(c->psiDzz);
+    free(c->fgx); free(c->fgy); free(c->fgz);
     free(c);
 }
 
@@ -197,6 +204,113 @@ static double l1_measure(const orc_ctx *c, const double *newv, const double *old
     return a / (c->p.dt * b);
 }
 
+/* Spectral second derivatives and the time derivative of psi for the surface diagnostics,
+ * from the spectrum psiq (times `sc`) and the nonlinear spectrum Nq of the same step:
+ *   dTpsi = iCT(sc (L psiq) + sN Nq), psiDaa = iCT(-sc q_a^2 psiq)
+ * noadv (psiq unscaled, sc = sN = scale): no-adv/cosNoAdvTrackSing.cpp:737-750,760-764;
+ * adv (psiq scaled, sc = 1, sN = scale): adv/cosAdvTrackMult.cpp:1311-1347. */
+static void surface_spectra(orc_ctx *c, double sc, double sN)
+{
+    const long n = c->n;
+    if (!c->dTpsi) {
+        c->dTpsi = dal(n); c->psiDxx = dal(n); c->psiDyy = dal(n); c->psiDzz = dal(n);
+    }
+    for (int i = 0; i < c->nx; i++)
+        for (int j = 0; j < c->ny; j++)
+            for (int k = 0; k < c->nz; k++) {
+                long q = IDX(c, i, j, k);
+                c->dTpsi[q] = sc == 1.0 ? (c->aLin[q] * c->psiq[q] + sN * c->Nq[q])
+                                        : sc * (c->aLin[q] * c->psiq[q] + c->Nq[q]);
+                c->psiDxx[q] = -sc * c->qx[i] * c->qx[i] * c->psiq[q];
+                c->psiDyy[q] = -sc * c->qy[j] * c->qy[j] * c->psiq[q];
+                c->psiDzz[q] = -sc * c->qz[k] * c->qz[k] * c->psiq[q];
+            }
+    r3(c, c->dTpsi, c->dTpsi, T01, T01, T01);
+    r3(c, c->psiDxx, c->psiDxx, T01, T01, T01);
+    r3(c, c->psiDyy, c->psiDyy, T01, T01, T01);
+    r3(c, c->psiDzz, c->psiDzz, T01, T01, T01);
+}
+
+/* Finite-difference gradient of psi, centred inside and one-sided (2 (a - b) / 2dx) at the
+ * walls: no-adv/cosNoAdvTrackSing.cpp:819-878. */
+static void fd_gradient(orc_ctx *c, const double *psi)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const double tdx = 2 * c->dx, tdy = 2 * c->dy, tdz = 2 * c->dz;
+    if (!c->fgx) { c->fgx = dal(c->n); c->fgy = dal(c->n); c->fgz = dal(c->n); }
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                long q = IDX(c, i, j, k);
+                if (i > 0 && i < nx - 1) c->fgx[q] = (psi[IDX(c, i + 1, j, k)] - psi[IDX(c, i - 1, j, k)]) / tdx;
+                else if (i == 0) c->fgx[q] = 2 * (psi[IDX(c, 1, j, k)] - psi[q]) / tdx;
+                else c->fgx[q] = 2 * (psi[q] - psi[IDX(c, i - 1, j, k)]) / tdx;
+                if (j != 0 && j != ny - 1) c->fgy[q] = (psi[IDX(c, i, j + 1, k)] - psi[IDX(c, i, j - 1, k)]) / tdy;
+                else if (j == 0) c->fgy[q] = 2 * (psi[IDX(c, i, j + 1, k)] - psi[q]) / tdy;
+                else c->fgy[q] = 2 * (psi[q] - psi[IDX(c, i, j - 1, k)]) / tdy;
+                if (k != 0 && k != nz - 1) c->fgz[q] = (psi[q + 1] - psi[q - 1]) / tdz;
+                else if (k == 0) c->fgz[q] = 2 * (psi[q + 1] - psi[q]) / tdz;
+                else c->fgz[q] = 2 * (psi[q] - psi[q - 1]) / tdz;
+            }
+}
+
+/* Interface per (i, j) column, scanning z downward (first psi > 0.7, then first psi < 0,
+ * the nearer of k, k+1), with the normal velocity dTpsi/|grad psi| and the curvatures 2H, K
+ * (Megrabov's divergence forms) there: no-adv/cosNoAdvTrackSing.cpp:880-964,
+ * adv/cosAdvTrackMult.cpp:1417-1515.  Mixed derivatives are differences of the gradient
+ * fields: along y at the chosen index k2, along z around that index with the branch taken
+ * on k (as the reference does).  An element past the end of the array reads 0. */
+static void surface_eval(orc_ctx *c, const double *psi, const double *gx, const double *gy, const double *gz)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const double tdy = 2 * c->dy, tdz = 2 * c->dz;
+    const long n = c->n;
+#define GAT(f, q) ((q) < n ? (f)[q] : 0.0)
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++) {
+            const long col = (long)i * ny + j;
+            c->s_idx[col] = -1;
+            c->s_vel[col] = c->s_H[col] = c->s_K[col] = NAN;
+            int track = 0;
+            for (int k = nz - 1; k > -1; k--) {
+                long index = IDX(c, i, j, k);
+                if (psi[index] > 0.7 && track == 0) track = 1;
+                if (psi[index] < 0.0 && track == 1) {
+                    int k2 = k;
+                    if (fabs(psi[index]) > fabs(psi[index + 1])) { index = index + 1; k2 = k + 1; }
+                    c->s_idx[col] = k2;
+                    const double gxv = gx[index], gyv = gy[index], gzv = gz[index];
+                    const double gradVal = sqrt(gxv * gxv + gyv * gyv + gzv * gzv);
+                    c->s_vel[col] = c->dTpsi[index] / gradVal;
+                    double Dxy = 0, Dxz = 0, Dyz = 0;
+                    if (j > 0 && j < ny - 1) Dxy = (gx[IDX(c, i, j + 1, k2)] - gx[IDX(c, i, j - 1, k2)]) / tdy;
+                    if (j == 0) Dxy = 2 * (gx[IDX(c, i, 1, k2)] - gx[IDX(c, i, 0, k2)]) / tdy;
+                    if (j == ny - 1) Dxy = 2 * (gx[IDX(c, i, j, k2)] - gx[IDX(c, i, j - 1, k2)]) / tdy;
+                    if (k > 0 && k < nz - 1) {
+                        Dxz = (GAT(gx, index + 1) - gx[index - 1]) / tdz;
+                        Dyz = (GAT(gy, index + 1) - gy[index - 1]) / tdz;
+                    }
+                    if (k == 0) {
+                        Dxz = 2 * (GAT(gx, index + 1) - gx[index]) / tdz;
+                        Dyz = 2 * (GAT(gy, index + 1) - gy[index]) / tdz;
+                    }
+                    const double Dxx = c->psiDxx[index], Dyy = c->psiDyy[index], Dzz = c->psiDzz[index];
+                    c->s_H[col] = ((gyv * gyv + gzv * gzv) * Dxx + (gxv * gxv + gzv * gzv) * Dyy +
+                                   (gxv * gxv + gyv * gyv) * Dzz -
+                                   2 * (gxv * gyv * Dxy + gxv * gzv * Dxz + gyv * gzv * Dyz)) /
+                                  pow(gradVal, 3);
+                    c->s_K[col] = (gzv * gzv * (Dxx * Dyy - Dxy * Dxy) + gxv * gxv * (Dyy * Dzz - Dyz * Dyz) +
+                                   gyv * gyv * (Dxx * Dzz - Dxz * Dxz) +
+                                   2 * (gyv * Dxy * (gzv * Dxz - gxv * Dzz) + gxv * Dxz * (gyv * Dyz - gzv * Dyy) +
+                                        gzv * Dyz * (gxv * Dxy - gyv * Dxx))) /
+                                  pow(gradVal, 4);
+                    track = 2;
+                }
+            }
+        }
+#undef GAT
+}
+
 /* ---------------- noadv: no-adv/cosNoAdvTrackSing.cpp:681-764,1072 ---------------- */
 static void step_noadv(orc_ctx *c)
 {
@@ -206,10 +320,15 @@ static void step_noadv(orc_ctx *c)
     nonlin(c, c->psi, c->Nr);                                      /* :713-723 */
     r3(c, c->Nr, c->Nq, T10, T10, T10);                            /* :727 */
     r3(c, c->psi, c->psiq, T10, T10, T10);                         /* :731 */
+    if (c->surf_pending) surface_spectra(c, c->scale, c->scale);   /* :737-750 */
     for (long q = 0; q < n; q++)                                   /* :752-753 */
         c->psiq[q] = c->scale * (c->C1[q] * c->psiq[q] + dtd2 * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
     r3(c, c->psiq, c->psiNew, T01, T01, T01);                      /* :758 */
     c->L1 = l1_measure(c, c->psiNew, c->psi);                      /* :769-789 */
+    if (c->surf_pending) {                                         /* :808-964, on psi^n */
+        fd_gradient(c, c->psi);
+        surface_eval(c, c->psi, c->fgx, c->fgy, c->fgz);
+    }
     memcpy(c->psi, c->psiNew, sizeof(double) * n);                 /* :1072 */
 }
 
@@ -305,10 +424,12 @@ static void step_adv(orc_ctx *c)
         c->Nr[q] = b * pow(c->psi[q], 3) - g * pow(c->psi[q], 5) - c->vx[q] * c->gx[q] -
                    c->vy[q] * c->gy[q] - c->vz[q] * c->gz[q];
     r3(c, c->Nr, c->Nq, T10, T10, T10);                             /* :1307 */
+    if (c->surf_pending) surface_spectra(c, 1.0, c->scale);         /* :1311-1347 */
     for (long q = 0; q < n; q++)                                    /* :1355-1365 */
         c->psiq[q] = (c->C1[q] * c->psiq[q] + dtd2 * c->scale * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
     r3(c, c->psiq, c->psiNew, T01, T01, T01);                       /* :1369 */
     c->L1 = l1_measure(c, c->psiNew, c->psi);                       /* :1374-1396 */
+    if (c->surf_pending) surface_eval(c, c->psi, c->gx, c->gy, c->gz); /* :1417-1515, psi^n */
     memcpy(c->psi, c->psiNew, sizeof(double) * n);                  /* :1742 */
 }
 
@@ -421,6 +542,17 @@ int orc_step(orc_ctx *c, int nsteps)
         else step_quasi(c);
     }
     return 0;
+}
+
+int orc_step_surface(orc_ctx *c, int *surf, double *vel, double *curvH, double *curvK)
+{
+    if (!c || !c->have_psi || c->p.model == ORC_QUASI || !surf || !vel || !curvH || !curvK) return -1;
+    c->s_idx = surf; c->s_vel = vel; c->s_H = curvH; c->s_K = curvK;
+    c->surf_pending = 1;
+    int rc = orc_step(c, 1);
+    c->surf_pending = 0;
+    c->s_idx = NULL; c->s_vel = c->s_H = c->s_K = NULL;
+    return rc;
 }
 
 int orc_get(const orc_ctx *c, int field, double *out)

@@ -55,6 +55,13 @@ void orc_destroy(orc_ctx *c);
 int orc_set_psi(orc_ctx *c, const double *psi);
 /* Advances nsteps time steps (the reference's loop body). */
 int orc_step(orc_ctx *c, int nsteps);
+/* One time step that also evaluates the surface diagnostics the reference writes every
+ * 1000 steps (noadv, adv): per (i, j) column (nx*ny entries) the flat-tracked interface
+ * index along z (-1: none), the normal velocity dTpsi/|grad psi| and the curvatures 2H and
+ * K there (NaN: none), all at the step's starting state psi^n: noadv
+ * no-adv/cosNoAdvTrackSing.cpp:737-964 (finite-difference gradient), adv
+ * adv/cosAdvTrackMult.cpp:1311-1347,1417-1515 (the step's spectral gradient). */
+int orc_step_surface(orc_ctx *c, int *surf, double *vel, double *curvH, double *curvK);
 /* Copies one field (nx*ny*nz doubles) out. */
 int orc_get(const orc_ctx *c, int field, double *out);
 /* diag[0]=L1 of the last step (ref definition), diag[1]=mass (quasi), diag[2]=energy of the

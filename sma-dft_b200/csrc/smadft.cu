@@ -30,6 +30,7 @@ struct smadft_ctx {
     Ctx c;
     std::map<int, StepGraph> graphs;
     bool use_graphs = true;
+    SurfaceScratch surf;
 };
 
 namespace {
@@ -403,6 +404,12 @@ int smadft_destroy(smadft_ctx *h)
     if (c.red) cudaFree(c.red);
     if (c.red_out) cudaFree(c.red_out);
     if (c.stage) cudaFree(c.stage);
+    cudaFree(h->surf.psih_prev);
+    cudaFree(h->surf.fields);
+    cudaFree(h->surf.idx);
+    cudaFree(h->surf.vel);
+    cudaFree(h->surf.curvH);
+    cudaFree(h->surf.curvK);
     for (int m = 0; m < Ctx::kMaxFork; m++) {
         if (c.aux[m]) cudaStreamDestroy(c.aux[m]);
         if (c.ev_join[m]) cudaEventDestroy(c.ev_join[m]);
@@ -533,6 +540,39 @@ int smadft_step_diag(smadft_ctx *h, smadft_diag *out)
     cudaSetDevice(c.dev);
     std::memset(out, 0, sizeof(*out));
     return c.f32 ? step_diag_t<float>(c, out) : step_diag_t<double>(c, out);
+}
+
+int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH, double *curvK)
+{
+    if (!h || !surf_idx || !vel || !curvH || !curvK) return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
+    if (c.p.model == SMADFT_MODEL_QUASI) return fail(c, SMADFT_ERR_UNSUPPORTED, "surface diagnostics: noadv and adv");
+    cudaSetDevice(c.dev);
+    SurfaceScratch &sc = h->surf;
+    const size_t cols = (size_t)c.g.nx * c.g.ny;
+    if (!sc.psih_prev) {
+        bool ok = cudaMalloc(&sc.psih_prev, sizeof(double) * c.n) == cudaSuccess &&
+                  cudaMalloc(&sc.fields, 4 * c.esize * c.n) == cudaSuccess &&
+                  cudaMalloc(&sc.idx, sizeof(int) * cols) == cudaSuccess &&
+                  cudaMalloc(&sc.vel, sizeof(double) * cols) == cudaSuccess &&
+                  cudaMalloc(&sc.curvH, sizeof(double) * cols) == cudaSuccess &&
+                  cudaMalloc(&sc.curvK, sizeof(double) * cols) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            return fail(c, SMADFT_ERR_NOMEM, "surface diagnostics scratch");
+        }
+    }
+    int rc = c.f32 ? surface_step<float>(c, sc) : surface_step<double>(c, sc);
+    if (rc) return rc;
+    c.steps++;
+    c.psi_current = (c.p.model != SMADFT_MODEL_ADV);
+    SMADFT_CUDA(cudaMemcpyAsync(surf_idx, sc.idx, sizeof(int) * cols, cudaMemcpyDeviceToHost, c.stream));
+    SMADFT_CUDA(cudaMemcpyAsync(vel, sc.vel, sizeof(double) * cols, cudaMemcpyDeviceToHost, c.stream));
+    SMADFT_CUDA(cudaMemcpyAsync(curvH, sc.curvH, sizeof(double) * cols, cudaMemcpyDeviceToHost, c.stream));
+    SMADFT_CUDA(cudaMemcpyAsync(curvK, sc.curvK, sizeof(double) * cols, cudaMemcpyDeviceToHost, c.stream));
+    SMADFT_CUDA(cudaStreamSynchronize(c.stream));
+    return SMADFT_OK;
 }
 
 int smadft_sync(smadft_ctx *h)

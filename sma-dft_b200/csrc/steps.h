@@ -26,4 +26,14 @@ template <typename T> int plain_pass(Ctx &c, const T *in, T *out, int axis, int 
 // quasi diagnostics sums: ms[0] = sum rho, ms[1] = sum e
 template <typename T> int reduce_mass_energy(Ctx &c, double *ms);
 
+// device scratch of smadft_step_surface (allocated on first use)
+struct SurfaceScratch {
+    double *psih_prev = nullptr;   // psihat^n (n doubles)
+    void *fields = nullptr;        // dTpsi, psi_xx, psi_yy, psi_zz (4 n elements of the field type)
+    int *idx = nullptr;            // per column: interface index along z (nx ny)
+    double *vel = nullptr, *curvH = nullptr, *curvK = nullptr;
+};
+// one loop body with the interface diagnostics (surface.cu; noadv, adv)
+template <typename T> int surface_step(Ctx &c, SurfaceScratch &sc);
+
 }  // namespace smadft

@@ -87,6 +87,7 @@ SIGNATURES = [
     ("smadft_track", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                     ctypes.c_double, _P(ctypes.c_int), _dp]),
     ("smadft_free_energy", ctypes.c_int, [_vp, _dp]),
+    ("smadft_step_surface", ctypes.c_int, [_vp, _P(ctypes.c_int), _dp, _dp, _dp]),
     ("smadft_save_checkpoint", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("smadft_load_checkpoint", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("smadft_r2r3d_device", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
@@ -255,6 +256,16 @@ class Solver:
         _check(lib().smadft_track(self._h, FIELD[field], axis, mode, hi, lo,
                                   idx.ctypes.data_as(_P(ctypes.c_int)), _dptr(pos)), self._h)
         return idx, pos
+
+    def step_surface(self):
+        """One step with the interface diagnostics: per (i, j) column the interface index
+        along z (-1: none), normal velocity, 2H and K (NaN: none), shaped (nx, ny)."""
+        shp = (self.shape[0], self.shape[1])
+        idx = np.empty(shp, dtype=np.int32)
+        vel, h, k = (np.empty(shp) for _ in range(3))
+        _check(lib().smadft_step_surface(self._h, idx.ctypes.data_as(_P(ctypes.c_int)), _dptr(vel), _dptr(h),
+                                         _dptr(k)), self._h)
+        return idx, vel, h, k
 
     def save(self, path: str) -> None:
         _check(lib().smadft_save_checkpoint(self._h, path.encode()), self._h)

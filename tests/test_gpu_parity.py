@@ -261,3 +261,47 @@ def test_config2_noadv_256_fp32_interface_error():
     assert found.sum() > 0.5 * found.size
     lam0_cells = p.nw                      # lambda0 = nw grid cells
     assert np.max(np.abs(pa[found] - pb[found])) / lam0_cells <= 0.01
+
+
+@pytest.mark.parametrize("model,shape,kw", [
+    (smadft.NOADV, (16, 12, 40), dict(dt=0.05, eps=-0.7)),
+    (smadft.ADV, (16, 12, 40), dict(dt=0.02, eps=-0.7)),
+    (smadft.ADV, (12, 64, 64), dict(dt=0.01, eps=-0.7)),
+])
+@pytest.mark.parametrize("precision,tol", [(smadft.FP64, 1e-9), (smadft.FP32, 2e-3)], ids=["fp64", "fp32"])
+def test_step_surface_matches_oracle(model, shape, kw, precision, tol):
+    """Interface diagnostics (index, normal velocity, 2H, K per column) against the oracle
+    after 20 steps; the oracle's diagnostics are pinned to the reference's output files."""
+    p = smadft.params(model, shape, precision=precision, **kw)
+    z = np.arange(shape[2]) * 2 * np.pi / 8
+    rng = np.random.default_rng(7)
+    psi0 = (1.3 * np.cos(z)[None, None, :] * np.ones((shape[0], shape[1], 1))
+            + 0.05 * np.sin(np.arange(shape[0]) * 0.7)[:, None, None] * np.cos(np.arange(shape[1]) * 0.5)[None, :, None]
+            + 0.01 * rng.standard_normal(shape))
+    o = oracle.Oracle(OMODEL[model], shape, nw=p.nw, dt=p.dt, eps=p.eps, nu=p.nu)
+    o.set_psi(psi0)
+    o.step(20)
+    oi, ov, oh, ok = o.step_surface()
+    with smadft.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(20)
+        gi, gv, gh, gk = s.step_surface()
+        after = s.get("psi")
+    o_after = o.get(oracle.F_PSI)
+    found = oi >= 0
+    assert found.sum() > oi.size // 2
+    agree = gi == oi
+    assert agree.mean() >= (1.0 if precision == smadft.FP64 else 0.99)
+    m = found & agree
+    for got, want in ((gv, ov), (gh, oh), (gk, ok)):
+        assert np.max(np.abs(got[m] - want[m])) <= tol * np.max(np.abs(want[m]))
+    assert rel_max(after, o_after) <= (1e-10 if precision == smadft.FP64 else 1e-4)
+
+
+def test_step_surface_quasi_unsupported():
+    p = smadft.params(smadft.QUASI, (16, 16, 16), dt=0.002)
+    with smadft.Solver(p) as s:
+        s.set_psi(np.zeros((16, 16, 16)))
+        with pytest.raises(smadft.SmadftError) as e:
+            s.step_surface()
+        assert e.value.code == -6

@@ -110,3 +110,36 @@ def test_reference_focal_conic_ic_matches_builder(smadft_lib):
     p = smadft.params(smadft.ADV, shape, nw=16.0)
     ours = smadft.ic_focal_conic(p, A=1.328, radius=10.0)   # argv radius 10, Amp 1.328
     assert np.max(np.abs(ours - fields["psi"])) == 0.0
+
+
+def _smectic_ic(shape, seed):
+    nz = shape[2]
+    z = np.arange(nz) * 2 * np.pi / 8
+    rng = np.random.default_rng(seed)
+    return (1.3 * np.cos(z)[None, None, :] * np.ones((shape[0], shape[1], 1))
+            + 0.05 * np.sin(np.arange(shape[0]) * 0.7)[:, None, None] * np.cos(np.arange(shape[1]) * 0.5)[None, :, None]
+            + 0.01 * rng.standard_normal(shape))
+
+
+@needs_ref
+@pytest.mark.parametrize("which,params", [
+    ("noadv", dict(nw=8, dt=0.05, eps=-0.7)),
+    ("adv", dict(nw=8, dt=0.02, eps=-0.7, nu=1.0)),
+])
+def test_oracle_surface_matches_live_reference(which, params):
+    """surfPsi / velSurf / curvH / curvK written by the reference at step 1000
+    (no-adv/cosNoAdvTrackSing.cpp:808-1021, adv/cosAdvTrackMult.cpp:1311-1585)."""
+    shape = (16, 12, 20)
+    psi0 = _smectic_ic(shape, 5)
+    _, texts, _ = oracle.run_reference(which, shape, 1000, psi0=psi0, **params)
+    ref = {n: np.array([float(x) for x in texts[n + ".dat"].split()]) for n in ("surfPsi", "velSurf", "curvH", "curvK")}
+    o = oracle_for(which, shape, params)
+    o.set_psi(psi0)
+    o.step(999)
+    idx, vel, h, k = o.step_surface()
+    found = idx.reshape(-1) >= 0
+    assert found.sum() > idx.size // 2
+    assert np.array_equal(idx.reshape(-1)[found].astype(float), ref["surfPsi"][found])
+    for name, mine in (("velSurf", vel), ("curvH", h), ("curvK", k)):
+        a, b = mine.reshape(-1)[found], ref[name][found]
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b)), name
