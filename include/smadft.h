@@ -149,10 +149,13 @@ int smadft_track(smadft_ctx *ctx, int field, int axis, int mode, double hi, doub
  * i*ny + j) the flat-tracked interface index along z (-1: none), the normal velocity
  * dTpsi/|grad psi| and the curvatures 2H and K (Megrabov's divergence forms) there (NaN:
  * none), all at the step's starting state; noadv uses the finite-difference gradient of
- * psi, adv the step's spectral gradient.  Replaces no-adv/cosNoAdvTrackSing.cpp:737-764,
- * 808-1021 and adv/cosAdvTrackMult.cpp:1311-1347,1417-1585.  noadv and adv only
- * (SMADFT_ERR_UNSUPPORTED for quasi).  Synchronises. */
-int smadft_step_surface(smadft_ctx *ctx, int *surf_idx, double *vel, double *curvH, double *curvK);
+ * psi, adv the step's spectral gradient.  diag (may be NULL) receives the step's FP64
+ * diagnostics as smadft_step_diag gives them, since the reference computes both on the same
+ * iteration.  Replaces no-adv/cosNoAdvTrackSing.cpp:737-764,808-1021 and
+ * adv/cosAdvTrackMult.cpp:1311-1347,1417-1585.  noadv and adv only (SMADFT_ERR_UNSUPPORTED
+ * for quasi).  Synchronises. */
+int smadft_step_surface(smadft_ctx *ctx, int *surf_idx, double *vel, double *curvH, double *curvK,
+                        smadft_diag *diag);
 /* Free energy of the current psi, sum(e) dx^3 with the quasi energy density
  * (quasi/quasi.cpp:1470-1473) for any model; FP64 reduction. */
 int smadft_free_energy(smadft_ctx *ctx, double *out);

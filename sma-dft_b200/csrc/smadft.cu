@@ -171,6 +171,9 @@ int ensure_psi(Ctx &c)
 }
 
 template <typename T>
+int finish_diag(Ctx &c, smadft_diag *out);
+
+template <typename T>
 int step_diag_t(Ctx &c, smadft_diag *out)
 {
     int rc;
@@ -183,6 +186,15 @@ int step_diag_t(Ctx &c, smadft_diag *out)
     } else {
         if ((rc = one_step<T>(c, true))) return rc;
     }
+    return finish_diag<T>(c, out);
+}
+
+// After a loop body that left psi^n in S_PSI and psi^{n+1} in S_PSI2: FP64 L1 / mean (and
+// quasi's mass and energy) of the step, then psi^{n+1} -> S_PSI.
+template <typename T>
+int finish_diag(Ctx &c, smadft_diag *out)
+{
+    int rc;
     c.steps++;
     double sums[4];
     const T *nw = c.f<T>(S_PSI2), *od = c.f<T>(S_PSI);
@@ -202,6 +214,16 @@ int step_diag_t(Ctx &c, smadft_diag *out)
     out->energy = ms[1] * dx3;
     out->steps = c.steps;
     return out->nonfinite ? fail(c, SMADFT_ERR_NONFINITE, "psi is not finite") : SMADFT_OK;
+}
+
+// the surface body, then the step's L1 diagnostics (psi^{n+1} -> S_PSI as in step_diag)
+template <typename T>
+int step_surface_t(Ctx &c, SurfaceScratch &sc, smadft_diag *d)
+{
+    int rc = surface_step<T>(c, sc);
+    if (rc) return rc;
+    if (c.p.model == SMADFT_MODEL_ADV && (rc = refresh_psi<T>(c, c.f<T>(S_PSI2)))) return rc;
+    return finish_diag<T>(c, d);
 }
 
 template <typename T>
@@ -542,7 +564,8 @@ int smadft_step_diag(smadft_ctx *h, smadft_diag *out)
     return c.f32 ? step_diag_t<float>(c, out) : step_diag_t<double>(c, out);
 }
 
-int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH, double *curvK)
+int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH, double *curvK,
+                        smadft_diag *diag)
 {
     if (!h || !surf_idx || !vel || !curvH || !curvK) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
@@ -563,16 +586,17 @@ int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH
             return fail(c, SMADFT_ERR_NOMEM, "surface diagnostics scratch");
         }
     }
-    int rc = c.f32 ? surface_step<float>(c, sc) : surface_step<double>(c, sc);
-    if (rc) return rc;
-    c.steps++;
-    c.psi_current = (c.p.model != SMADFT_MODEL_ADV);
+    smadft_diag d;
+    std::memset(&d, 0, sizeof(d));
+    int rc = c.f32 ? step_surface_t<float>(c, sc, &d) : step_surface_t<double>(c, sc, &d);
+    if (rc && rc != SMADFT_ERR_NONFINITE) return rc;
+    if (diag) *diag = d;
     SMADFT_CUDA(cudaMemcpyAsync(surf_idx, sc.idx, sizeof(int) * cols, cudaMemcpyDeviceToHost, c.stream));
     SMADFT_CUDA(cudaMemcpyAsync(vel, sc.vel, sizeof(double) * cols, cudaMemcpyDeviceToHost, c.stream));
     SMADFT_CUDA(cudaMemcpyAsync(curvH, sc.curvH, sizeof(double) * cols, cudaMemcpyDeviceToHost, c.stream));
     SMADFT_CUDA(cudaMemcpyAsync(curvK, sc.curvK, sizeof(double) * cols, cudaMemcpyDeviceToHost, c.stream));
     SMADFT_CUDA(cudaStreamSynchronize(c.stream));
-    return SMADFT_OK;
+    return rc;
 }
 
 int smadft_sync(smadft_ctx *h)

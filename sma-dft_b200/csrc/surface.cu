@@ -169,10 +169,7 @@ int surface_step(Ctx &c, SurfaceScratch &sc)
         f[0], f[1], f[2], f[3], sc.idx, sc.vel, sc.curvH, sc.curvK);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
-    if (fd) {
-        SMADFT_CUDA(cudaMemcpyAsync(c.slot[S_PSI], c.slot[S_PSI2], c.esize * c.n, cudaMemcpyDeviceToDevice, c.stream));
-    }
-    return SMADFT_OK;
+    return SMADFT_OK;   // noadv: psi^{n+1} waits in S_PSI2 (the caller moves it to S_PSI)
 }
 
 #if !defined(SMADFT_INST_DOUBLE)

@@ -2,8 +2,8 @@
 //
 // It keeps the reference's driver surface (parameter block, IC builders, output files) and
 // calls the library once per loop body.  Output files follow the reference's names and
-// text formats: L1.dat (no-adv/cosNoAdvTrackSing.cpp:789-795), surfPsi.dat, psiMid.dat
-// (:1004-1030), vx/vy/vz.dat mid slices (adv/cosAdvTrackMult.cpp:1613-1731), mass.dat and
+// text formats: L1.dat (no-adv/cosNoAdvTrackSing.cpp:789-795), surfPsi.dat, velSurf.dat,
+// curvH.dat, curvK.dat, psiMid.dat (:1004-1030), vx/vy/vz.dat mid slices (adv/cosAdvTrackMult.cpp:1613-1731), mass.dat and
 // energy.dat (quasi/quasi.cpp:2232-2248), info (quasi/quasi.cpp:820-843), and the per-rank
 // text save psi0.dat (adv/cosAdvTrackMult.cpp:1546-1557) which `ic=file:` reads back.
 //
@@ -133,6 +133,8 @@ int main(int argc, char **argv)
 
     {   // files are created empty, as the reference does at start-up
         for (const char *f : {"L1.dat", "psiMid.dat", "surfPsi.dat"}) std::ofstream(out + f).close();
+        if (m != SMADFT_MODEL_QUASI)
+            for (const char *f : {"velSurf.dat", "curvH.dat", "curvK.dat"}) std::ofstream(out + f).close();
         if (m != SMADFT_MODEL_NOADV) for (const char *f : {"vx.dat", "vy.dat", "vz.dat"}) std::ofstream(out + f).close();
         if (m == SMADFT_MODEL_QUASI) for (const char *f : {"mass.dat", "energy.dat"}) std::ofstream(out + f).close();
         std::ofstream info(out + "info");
@@ -146,13 +148,19 @@ int main(int argc, char **argv)
     std::vector<double> field(N);
     const int na = taxis == 0 ? p.ny : p.nx, nb = taxis == 2 ? p.ny : p.nz;
     std::vector<int> sidx((size_t)na * nb);
-    std::vector<double> spos((size_t)na * nb);
+    std::vector<double> spos((size_t)na * nb), vel((size_t)na * nb), cH((size_t)na * nb), cK((size_t)na * nb);
+    // the reference's own save iteration (z-scanning flat tracker, noadv / adv) also writes the
+    // normal velocity and curvatures of that step (no-adv/cosNoAdvTrackSing.cpp:808-1021,
+    // adv/cosAdvTrackMult.cpp:1311-1585)
+    const bool with_surface = m != SMADFT_MODEL_QUASI && taxis == 2 && tmode == SMADFT_TRACK_FLAT;
     while (done < steps) {
         long chunk = std::min<long>(l1every - 1, steps - done - 1);
         if (chunk > 0 && (rc = smadft_step(ctx, (int)chunk))) return die("smadft_step", rc, ctx);
         done += chunk;
         smadft_diag d;
-        rc = smadft_step_diag(ctx, &d);
+        const bool surf_iter = with_surface && countSave + 1 == saveevery;
+        rc = surf_iter ? smadft_step_surface(ctx, sidx.data(), vel.data(), cH.data(), cK.data(), &d)
+                       : smadft_step_diag(ctx, &d);
         done++;
         if (rc == SMADFT_ERR_NONFINITE) {
             std::fprintf(stderr, "smadft_run: psi became non-finite at step %ld\n", done);
@@ -167,11 +175,20 @@ int main(int argc, char **argv)
         if (++countSave == saveevery) {
             countSave = 0;
             int fld = (m == SMADFT_MODEL_QUASI && tmode == SMADFT_TRACK_LEVEL) ? SMADFT_FIELD_RHO : SMADFT_FIELD_PSI;
-            if ((rc = smadft_track(ctx, fld, taxis, tmode, thi, tlo, sidx.data(), spos.data())))
+            if (!surf_iter && (rc = smadft_track(ctx, fld, taxis, tmode, thi, tlo, sidx.data(), spos.data())))
                 return die("smadft_track", rc, ctx);
             {
                 std::ofstream s(out + "surfPsi.dat", std::ios_base::app);
                 for (size_t q = 0; q < sidx.size(); q++) s << sidx[q] << "\n";
+            }
+            if (surf_iter) {
+                const std::vector<double> *v[3] = {&vel, &cH, &cK};
+                const char *names[3] = {"velSurf.dat", "curvH.dat", "curvK.dat"};
+                for (int c = 0; c < 3; c++) {
+                    std::ofstream s(out + names[c], std::ios_base::app);
+                    s << std::setprecision(17);
+                    for (double x : *v[c]) s << x << "\n";
+                }
             }
             if ((rc = smadft_get_psi(ctx, field.data(), N))) return die("smadft_get_psi", rc, ctx);
             append_slice(out + "psiMid.dat", field, p.nx, p.ny, p.nz);

@@ -87,7 +87,7 @@ SIGNATURES = [
     ("smadft_track", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                     ctypes.c_double, _P(ctypes.c_int), _dp]),
     ("smadft_free_energy", ctypes.c_int, [_vp, _dp]),
-    ("smadft_step_surface", ctypes.c_int, [_vp, _P(ctypes.c_int), _dp, _dp, _dp]),
+    ("smadft_step_surface", ctypes.c_int, [_vp, _P(ctypes.c_int), _dp, _dp, _dp, _P(Diag)]),
     ("smadft_save_checkpoint", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("smadft_load_checkpoint", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("smadft_r2r3d_device", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
@@ -263,8 +263,10 @@ class Solver:
         shp = (self.shape[0], self.shape[1])
         idx = np.empty(shp, dtype=np.int32)
         vel, h, k = (np.empty(shp) for _ in range(3))
+        d = Diag()
         _check(lib().smadft_step_surface(self._h, idx.ctypes.data_as(_P(ctypes.c_int)), _dptr(vel), _dptr(h),
-                                         _dptr(k)), self._h)
+                                         _dptr(k), ctypes.byref(d)), self._h)
+        self.last_diag = d.as_dict()
         return idx, vel, h, k
 
     def save(self, path: str) -> None:

@@ -1,0 +1,66 @@
+"""The reference-style driver (sma-dft_b200/smadft_run) end to end: its output files against
+the oracle stepping the same initial condition.
+
+L1.dat gets one line per `l1every` steps (no-adv/cosNoAdvTrackSing.cpp:789-795); on the save
+iteration surfPsi.dat / velSurf.dat / curvH.dat / curvK.dat get one line per (i, j) column
+(:1004-1021, adv/cosAdvTrackMult.cpp:1578-1585).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "sma-dft_b200", "smadft_run")
+
+
+def read(path):
+    with open(path) as f:
+        return np.array([float(x) for x in f.read().split()])
+
+
+@pytest.mark.parametrize("model,omodel,extra", [
+    ("noadv", oracle.NOADV, dict(dt=0.05)),
+    ("adv", oracle.ADV, dict(dt=0.02, nu=1.0)),
+])
+def test_driver_outputs_match_oracle(tmp_path, model, omodel, extra):
+    if not os.path.exists(DRIVER):
+        pytest.skip("smadft_run not built")
+    shape = (16, 12, 20)
+    z = np.arange(shape[2]) * 2 * np.pi / 8
+    rng = np.random.default_rng(11)
+    psi0 = (1.3 * np.cos(z)[None, None, :] * np.ones((shape[0], shape[1], 1))
+            + 0.05 * np.sin(np.arange(shape[0]) * 0.7)[:, None, None] * np.cos(np.arange(shape[1]) * 0.5)[None, :, None]
+            + 0.01 * rng.standard_normal(shape))
+    ic = tmp_path / "ic.txt"
+    np.savetxt(ic, psi0.reshape(-1), fmt="%.17g")
+    args = [DRIVER, model, f"nx={shape[0]}", f"ny={shape[1]}", f"nz={shape[2]}", "nw=8", "eps=-0.7",
+            "steps=20", "l1every=10", "saveevery=2", f"ic=file:{ic}", f"out={tmp_path}"]
+    args += [f"{k}={v}" for k, v in extra.items()]
+    subprocess.run(args, check=True, capture_output=True, text=True)
+
+    o = oracle.Oracle(omodel, shape, nw=8, eps=-0.7, **extra)
+    o.set_psi(psi0)
+    o.step(10)
+    l1_10 = o.diag()["l1"]
+    o.step(9)
+    idx, vel, h, k = o.step_surface()
+    l1_20 = o.diag()["l1"]
+
+    l1 = read(tmp_path / "L1.dat")
+    assert l1.size == 2
+    assert np.allclose(l1, [l1_10, l1_20], rtol=1e-10, atol=0)
+    surf = read(tmp_path / "surfPsi.dat")
+    found = idx.reshape(-1) >= 0
+    assert found.sum() > found.size // 2
+    assert np.array_equal(surf, idx.reshape(-1).astype(float))
+    for name, want in (("velSurf.dat", vel), ("curvH.dat", h), ("curvK.dat", k)):
+        got = read(tmp_path / name)
+        w = want.reshape(-1)
+        assert np.max(np.abs(got[found] - w[found])) <= 1e-9 * np.max(np.abs(w[found])), name
+    final = read(tmp_path / "psi0.dat").reshape(shape)
+    assert np.max(np.abs(final - o.get(oracle.F_PSI))) <= 1e-10 * np.max(np.abs(final))

@@ -286,8 +286,10 @@ def test_step_surface_matches_oracle(model, shape, kw, precision, tol):
         s.set_psi(psi0)
         s.step(20)
         gi, gv, gh, gk = s.step_surface()
+        l1 = s.last_diag["l1"]
         after = s.get("psi")
     o_after = o.get(oracle.F_PSI)
+    assert abs(l1 - o.diag()["l1"]) <= (1e-10 if precision == smadft.FP64 else 1e-4) * abs(o.diag()["l1"])
     found = oi >= 0
     assert found.sum() > oi.size // 2
     agree = gi == oi
