@@ -599,6 +599,23 @@ int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH
     return rc;
 }
 
+int smadft_adjoint(smadft_ctx *h, const smadft_adj_opts *o, smadft_grads *out, double *d_psi0)
+{
+    if (!h || !o || !out || o->steps <= 0 || o->checkpoint_every <= 0 || o->axis < 0 || o->axis > 2 ||
+        (o->mode != SMADFT_TRACK_FLAT && o->mode != SMADFT_TRACK_BUMP))
+        return SMADFT_ERR_INVALID;
+    Ctx &c = h->c;
+    if (!c.have_psi || c.steps != 0) return fail(c, SMADFT_ERR_STATE, "adjoint: start from the initial condition");
+    if (c.p.model != SMADFT_MODEL_NOADV) return fail(c, SMADFT_ERR_UNSUPPORTED, "adjoint: noadv only");
+    cudaSetDevice(c.dev);
+    std::memset(out, 0, sizeof(*out));
+    int rc = c.f32 ? noadv_adjoint<float>(c, *o, out, d_psi0) : noadv_adjoint<double>(c, *o, out, d_psi0);
+    if (rc) return rc;
+    c.steps += o->steps;
+    c.psi_current = true;
+    return SMADFT_OK;
+}
+
 int smadft_sync(smadft_ctx *h)
 {
     if (!h) return SMADFT_ERR_INVALID;

@@ -35,5 +35,7 @@ struct SurfaceScratch {
 };
 // one loop body with the interface diagnostics (surface.cu; noadv, adv)
 template <typename T> int surface_step(Ctx &c, SurfaceScratch &sc);
+// adjoint of `o.steps` noadv loop bodies from the initial condition (adjoint.cu)
+template <typename T> int noadv_adjoint(Ctx &c, const smadft_adj_opts &o, smadft_grads *out, double *dpsi0_host);
 
 }  // namespace smadft

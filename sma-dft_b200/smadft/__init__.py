@@ -61,6 +61,18 @@ class Diag(ctypes.Structure):
                     steps=int(self.steps), nonfinite=int(self.nonfinite))
 
 
+class AdjOpts(ctypes.Structure):
+    """smadft_adj_opts"""
+    _fields_ = [("steps", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("axis", ctypes.c_int),
+                ("mode", ctypes.c_int), ("hi", ctypes.c_double), ("lo", ctypes.c_double)]
+
+
+class Grads(ctypes.Structure):
+    """smadft_grads"""
+    _fields_ = [("loss", ctypes.c_double), ("found", ctypes.c_int), ("d_eps", ctypes.c_double),
+                ("d_alpha", ctypes.c_double), ("d_beta", ctypes.c_double), ("d_gamma", ctypes.c_double)]
+
+
 class TuneReport(ctypes.Structure):
     """smadft_tune_report"""
     _fields_ = [("configs", ctypes.c_int), ("chosen", ctypes.c_int), ("ms", ctypes.c_double * 8)]
@@ -105,6 +117,7 @@ SIGNATURES = [
     ("smadft_batch_sync", ctypes.c_int, [_vp]),
     ("smadft_batch_last_error", ctypes.c_char_p, [_vp]),
     ("smadft_autotune", ctypes.c_int, [_vp, ctypes.c_int, _P(TuneReport)]),
+    ("smadft_adjoint", ctypes.c_int, [_vp, _P(AdjOpts), _P(Grads), _dp]),
     ("smadft_tune_config_name", ctypes.c_char_p, [ctypes.c_int]),
     ("smadft_ic_interface", ctypes.c_int, [_P(Params), ctypes.c_double, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_ulonglong, _dp]),
@@ -296,6 +309,17 @@ class Solver:
     def r2r_pass_device(self, src_ptr: int, dst_ptr: int, axis: int, kind: int) -> None:
         _check(lib().smadft_r2r_pass_device(self._h, _vp(src_ptr), _vp(dst_ptr), int(axis), int(kind)),
                self._h)
+
+    def adjoint(self, steps: int, checkpoint_every: int = 50, axis: int = 0, mode: int = TRACK_BUMP,
+                hi: float = 0.6, lo: float = 0.1, want_dpsi0: bool = True) -> dict:
+        """Interface-loss gradients of `steps` noadv loop bodies from the initial condition."""
+        o = AdjOpts(int(steps), int(checkpoint_every), int(axis), int(mode), float(hi), float(lo))
+        g = Grads()
+        dpsi = np.empty(self.shape, dtype=np.float64) if want_dpsi0 else None
+        _check(lib().smadft_adjoint(self._h, ctypes.byref(o), ctypes.byref(g),
+                                    _dptr(dpsi) if dpsi is not None else None), self._h)
+        return dict(loss=g.loss, found=g.found, eps=g.d_eps, alpha=g.d_alpha, beta=g.d_beta, gamma=g.d_gamma,
+                    psi0=dpsi)
 
     def autotune(self, steps: int = 5) -> dict:
         """Time each applicable kernel path on this run and keep the fastest (state kept)."""
