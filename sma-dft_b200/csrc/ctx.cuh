@@ -20,6 +20,10 @@
 
 namespace smadft {
 
+// Kernel attributes (dynamic shared memory opt-in) are per device: launch helpers keep one
+// flag per device index below this bound.
+constexpr int kMaxDevices = 64;
+
 // Field slots (allocated per model; unused slots stay null).
 enum Slot : int {
     S_PSI = 0, S_PSI2, S_PSIH, S_PSIH_OLD, S_NP, S_TMP,
@@ -166,11 +170,11 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
         tiles = (long long)(axis == 1 ? c.g.nx : c.g.ny) * a.tiles_b;
     }
     const size_t smem = 2 * (size_t)(a.W / 2) * a.ld * sizeof(cpx<T>);
-    static size_t attr_set = 0;   // largest opt-in so far, per template instantiation
-    if (smem > attr_set) {
+    static size_t attr_set[kMaxDevices] = {};   // largest opt-in so far, per device and instantiation
+    if (smem > attr_set[c.dev % kMaxDevices]) {
         SMADFT_CUDA(cudaFuncSetAttribute(r2r_pass_kernel<T, LD, ST>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = smem;
+        attr_set[c.dev % kMaxDevices] = smem;
     }
     r2r_pass_kernel<T, LD, ST><<<(unsigned)tiles, 256, smem, c.stream>>>(a, ld, st);
     SMADFT_CUDA(cudaGetLastError());
@@ -185,11 +189,11 @@ int launch_rd(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
     const int tiles_b = (c.g.nz + 31) / 32;
     const long long tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b * NC;
     constexpr size_t smem = rd_smem_bytes<T, N>();
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
+    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
         SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
+        attr_set |= 1ull << (c.dev % kMaxDevices);
     }
     r2r_rd_kernel<T, N, AXIS, LD, ST, NC><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         c.g, kinds, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
@@ -217,11 +221,11 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
         tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b;
     }
     constexpr size_t smem = fast_smem_bytes<T, N, CFG>();
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
+    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
         SMADFT_CUDA(cudaFuncSetAttribute(r2r_fast_kernel<T, N, AXIS, LD, ST, CFG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
+        attr_set |= 1ull << (c.dev % kMaxDevices);
     }
     r2r_fast_kernel<T, N, AXIS, LD, ST, CFG><<<(unsigned)tiles, CFG::THREADS, smem, c.stream>>>(
         c.g, kind, tiles_b, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), ld, st);
@@ -238,10 +242,10 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
     const int rows = c.g.nx * c.g.ny;
     const int tiles = (rows + 2 * kRdLines - 1) / (2 * kRdLines);
     constexpr size_t smem = rdz_smem_bytes<T, N>();
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
+    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
         SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
+        attr_set |= 1ull << (c.dev % kMaxDevices);
     }
     r2r_rdz_kernel<T, N><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h));
@@ -331,11 +335,11 @@ int launch_plane(Ctx &c, const PlaneKinds<NC> &kinds, LD ld, const StoreMulti<T,
     const PlanDev &pd = c.plans.at(N);
     constexpr size_t smem = plane_smem_bytes<T, N>();
     using ST = StoreMulti<T, NC>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
+    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
         SMADFT_CUDA(cudaFuncSetAttribute(r2r_plane_kernel<T, N, NC, LD, ST>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
+        attr_set |= 1ull << (c.dev % kMaxDevices);
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)c.g.nx * NC * PlaneInfo<N>::C);

@@ -96,6 +96,7 @@ struct LdNegLin {
 // S_c = (Sp2 - beta psi^3 + gamma psi^5) d_c psi (adv/cosAdvTrackMult.cpp:994-1015)
 template <typename T>
 struct LdForce {
+    static constexpr int kMinBlocks = 2;   // three fields per point: memory-bound, keep registers
     const T *__restrict__ psi, *__restrict__ sp2, *__restrict__ g;
     T beta, gamma;
     template <int V>
@@ -202,6 +203,7 @@ struct LdStokes {
 // N = beta psi^3 - gamma psi^5 - v . grad psi (adv/cosAdvTrackMult.cpp:1290-1303)
 template <typename T>
 struct LdAdvN {
+    static constexpr int kMinBlocks = 2;   // seven fields per point: memory-bound, keep registers
     const T *__restrict__ psi, *__restrict__ vx, *__restrict__ vy, *__restrict__ vz;
     const T *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
     T beta, gamma;

@@ -188,12 +188,20 @@ struct is_multi : std::false_type {};
 template <class X>
 struct is_multi<X, std::void_t<decltype(X::MULTI)>> : std::true_type {};
 
+// CTAs per SM a loader's FP32 register-direct pass is sized for: 3 unless the loader says
+// otherwise (kMinBlocks; the memory-bound many-field loaders keep more registers at 2)
+template <class X, class = void>
+struct ld_blocks { static constexpr int value = 3; };
+template <class X>
+struct ld_blocks<X, std::void_t<decltype(X::kMinBlocks)>> { static constexpr int value = X::kMinBlocks; };
+
 // NC loaders behind one component index (the index is uniform over a CTA)
 template <class... L>
 struct LoadMulti;
 template <class L0>
 struct LoadMulti<L0> {
     static constexpr bool MULTI = true;
+    static constexpr int kMinBlocks = ld_blocks<L0>::value;
     L0 h;
     template <int V, typename T>
     __device__ __forceinline__ void load(int, idx_t q, int i, int j, int k, T *out) const
@@ -207,6 +215,9 @@ struct LoadMulti<L0> {
 template <class L0, class L1, class... Ls>
 struct LoadMulti<L0, L1, Ls...> {
     static constexpr bool MULTI = true;
+    static constexpr int kMinBlocks = ld_blocks<L0>::value < ld_blocks<LoadMulti<L1, Ls...>>::value
+                                          ? ld_blocks<L0>::value
+                                          : ld_blocks<LoadMulti<L1, Ls...>>::value;
     L0 h;
     LoadMulti<L1, Ls...> t;
     template <int V, typename T>

@@ -45,10 +45,12 @@ struct RdInfo {
 template <typename T, int N>
 constexpr size_t rd_smem_bytes() { return ((size_t)kRdLines * RdInfo<N>::LD + 2 * N) * sizeof(cpx<T>); }
 
-// CTAs per SM the register budget is sized for: FP32 passes over a plain array fit three
-// (80 registers), the fused multi-field loaders and FP64 keep two
-template <typename T, class LD>
-constexpr int rd_min_blocks() { return (sizeof(T) == 4 && std::is_same<LD, LoadArr<T>>::value) ? 3 : 2; }
+// CTAs per SM the register budget is sized for: FP32 passes fit three (80 registers; the
+// fused loaders spill at most a few words there, and the extra resident CTA hides more
+// load latency) unless the loader asks for two (ld_blocks); FP64 passes, and FP32 passes
+// whose storer carries FP64 state reads (the spectral updates), keep two
+template <typename T, class LD, class ST>
+constexpr int rd_min_blocks() { return (sizeof(T) == 4 && sizeof(pre_t<ST, T>) == 4) ? ld_blocks<LD>::value : 2; }
 
 // natural sample index whose Makhoul position is p (inverse of makhoul_pos)
 template <int N>
@@ -327,7 +329,7 @@ struct RdPos {
 // NC > 1: multi-component pass (LoadMulti / StoreMulti); CTA b transforms component b mod NC
 // of tile b / NC, so the components' shared input reads meet in L2.
 template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
-__global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD>()) r2r_rd_kernel(Geom g, KindSet<NC> kinds, int tiles_b, LD ld,
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()) r2r_rd_kernel(Geom g, KindSet<NC> kinds, int tiles_b, LD ld,
                                                                        const cpx<T> *__restrict__ wt_g,
                                                                        const cpx<T> *__restrict__ ht_g, ST st)
 {
