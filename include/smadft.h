@@ -38,7 +38,8 @@ extern "C" {
 #define SMADFT_ERR_NONFINITE -4    /* psi became NaN/Inf (the reference's L1 test would
                                       silently stop: adv/cosAdvTrackMult.cpp:824)           */
 #define SMADFT_ERR_TIMEOUT -5      /* a bounded device wait ran out                         */
-#define SMADFT_ERR_UNSUPPORTED -6  /* grid length with a prime factor other than 2, 3, 5    */
+#define SMADFT_ERR_UNSUPPORTED -6  /* grid length with a prime factor other than 2, 3, 5,
+                                    * or a call the run's model does not have             */
 #define SMADFT_ERR_IO -7           /* checkpoint file could not be read or written          */
 #define SMADFT_ERR_STATE -8        /* call out of order (e.g. step before set_psi)          */
 #define SMADFT_ERR_NODEVICE -9     /* no CUDA device / extension not usable                 */
@@ -88,7 +89,11 @@ typedef struct {
     int divv_switch;    /* quasi: steps before div v comes from mass balance (ref 200) */
     int loaded;         /* quasi: the reference's load==1 branch (restart semantics)   */
     int device;         /* CUDA device ordinal                                        */
-    int reserved[5];
+    int conserved;      /* noadv, adv: 1 = conserved dynamics, the reference's
+                         * no-adv/cosNoAdvConserv.cpp (L and N weighted by q^2) and
+                         * adv/cosAdvConSingle.cpp (C1, C2 and the SH part of N weighted by
+                         * q^2, the advection v.grad psi not); 0 = the non-conserved models */
+    int reserved[4];
 } smadft_params;
 
 /* FP64 diagnostics of one step (no-adv/cosNoAdvTrackSing.cpp:769-801,
@@ -152,8 +157,11 @@ int smadft_track(smadft_ctx *ctx, int field, int axis, int mode, double hi, doub
  * psi, adv the step's spectral gradient.  diag (may be NULL) receives the step's FP64
  * diagnostics as smadft_step_diag gives them, since the reference computes both on the same
  * iteration.  Replaces no-adv/cosNoAdvTrackSing.cpp:737-764,808-1021 and
- * adv/cosAdvTrackMult.cpp:1311-1347,1417-1585.  noadv and adv only (SMADFT_ERR_UNSUPPORTED
- * for quasi).  Synchronises. */
+ * adv/cosAdvTrackMult.cpp:1311-1347,1417-1585.  Non-conserved noadv and adv only
+ * (SMADFT_ERR_UNSUPPORTED for quasi and conserved runs: adv/cosAdvConSingle.cpp has these
+ * outputs commented out, :1316-1352,1454-1524, and no-adv/cosNoAdvConserv.cpp:816-847 takes
+ * its spectra from the updated, already normalised psihat with a second scale factor, so its
+ * files do not hold the physical quantities).  Synchronises. */
 int smadft_step_surface(smadft_ctx *ctx, int *surf_idx, double *vel, double *curvH, double *curvK,
                         smadft_diag *diag);
 /* Free energy of the current psi, sum(e) dx^3 with the quasi energy density
@@ -232,7 +240,8 @@ const char *smadft_batch_last_error(const smadft_batch *batch);
  * final psi, then runs the reverse sweep, re-running each segment from its checkpoint.  The
  * found set and crossing cells are held fixed (as a small central difference sees them).
  * d_psi0 (may be NULL) receives dloss/dpsi_0 (nx*ny*nz doubles).  The run continues from
- * the final state.  noadv only (SMADFT_ERR_UNSUPPORTED otherwise).  Synchronises. */
+ * the final state.  Non-conserved noadv only (SMADFT_ERR_UNSUPPORTED otherwise).
+ * Synchronises. */
 typedef struct {
     int steps;              /* loop bodies                                   */
     int checkpoint_every;   /* K: psihat / Nhat_prev kept every K steps       */

@@ -39,6 +39,7 @@ class OrcParams(ctypes.Structure):
         ("nu", ctypes.c_double),
         ("rho0", ctypes.c_double), ("kp", ctypes.c_double), ("amp", ctypes.c_double),
         ("divv_switch", ctypes.c_int), ("loaded", ctypes.c_int),
+        ("conserved", ctypes.c_int),
     ]
 
 
@@ -107,7 +108,7 @@ def r2r_3d(x, kinds) -> np.ndarray:
 
 
 DEFAULTS = dict(nw=8.0, dt=0.05, alpha=1.0, beta=2.0, gamma=1.0, eps=-0.75, q0=1.0, nu=1.0,
-                rho0=1.0, kp=0.0, amp=1.34164, divv_switch=200, loaded=0)
+                rho0=1.0, kp=0.0, amp=1.34164, divv_switch=200, loaded=0, conserved=0)
 
 
 class Oracle:
@@ -176,9 +177,12 @@ class Oracle:
 # ----------------------------------------------------------------------------------
 # The reference itself, compiled from its sources by build_ref.sh (single-rank shims).
 # ----------------------------------------------------------------------------------
-REF_BINARIES = {"noadv": "noadv_ref", "bump": "bump_ref", "adv": "adv_ref", "quasi": "quasi_ref"}
+REF_BINARIES = {"noadv": "noadv_ref", "bump": "bump_ref", "adv": "adv_ref", "quasi": "quasi_ref",
+                "noadvc": "noadvc_ref", "advc": "advc_ref"}
 REF_DUMPS = {
     "noadv": ["psi", "nq"],
+    "noadvc": ["psi", "nq"],
+    "advc": ["psi", "vx", "vy", "vz", "gx", "gy", "gz", "nq"],
     "bump": ["psi"],
     "adv": ["psi", "vx", "vy", "vz", "gx", "gy", "gz", "nq"],
     "quasi": ["psi", "rho", "p", "vx", "vy", "vz", "mu", "energy", "psiq"],
@@ -224,6 +228,12 @@ def run_reference(which: str, shape, steps: int, psi0=None, workdir: str | None 
         elif which == "quasi":
             argv += ["1", "75", "10", "0"]
             os.makedirs(os.path.join(wd, "r1-e0d75"), exist_ok=True)
+        elif which == "noadvc":
+            argv += ["75", "10", str(nx), "0"]      # e0d radius N load
+            os.makedirs(os.path.join(wd, "r75-r10"), exist_ok=True)
+        elif which == "advc":
+            argv += ["1", "75", "10", str(nx), "0"]  # nu e0d radius N load
+            os.makedirs(os.path.join(wd, "r1-e0d75-r10"), exist_ok=True)
         r = subprocess.run(argv, cwd=wd, env=env, capture_output=True, text=True, check=True)
         fields = {}
         for name in REF_DUMPS[which]:

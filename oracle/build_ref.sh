@@ -13,7 +13,7 @@
 #   * psiMid's hard-coded j = 256 (noadv Sing)        -> Ny/2 (in range for small grids)
 #   * L1/mass/energy/velSurf/curvH/curvK text output  -> 17 significant digits
 #   * before MPI::Finalize(), binary dumps of the final fields
-# Usage: oracle/build_ref.sh   (writes oracle/_ref/{noadv,bump,adv,quasi}_ref)
+# Usage: oracle/build_ref.sh   (writes oracle/_ref/{noadv,bump,adv,quasi,noadvc,advc}_ref)
 set -euo pipefail
 REF="${SMADFT_REFERENCE:-/root/reference}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
@@ -91,3 +91,22 @@ build quasi_ref quasi/quasi.cpp \
   -e "s|mass_output << rho_sum << |mass_output << std::setprecision(17) << rho_sum << |" \
   -e "s|energy_output << energy << |energy_output << std::setprecision(17) << energy << |" \
   -e "s|^\(\s*\)/\*\* Create output files \*\*/|\1refshim_load_ic(psi_local.data(), alloc_local);|"
+
+# no-adv/cosNoAdvConserv.cpp (conserved dynamics); argv = e0d radius N load
+DUMP='refshim_dump("psi", psi_local.data(), alloc_local); refshim_dump("nq", Nq_local.data(), alloc_local);'
+build noadvc_ref no-adv/cosNoAdvConserv.cpp \
+  -e "s/const ptrdiff_t Nx = atof(argv\[3\]), Ny = atof(argv\[3\]), Nz = atof(argv\[3\]);/const ptrdiff_t Nx = (ptrdiff_t)$P(\"NX\", 64), Ny = (ptrdiff_t)$P(\"NY\", 64), Nz = (ptrdiff_t)$P(\"NZ\", 64);/" \
+  -e "s/const double ep = -0.01\*ep_arg;/const double ep = $P(\"EPS\", -0.01*ep_arg);/" \
+  -e "s|std::string strLoad = \"[^\"]*\";|std::string strLoad = std::string(refshim_dir()) + \"/r\";|" \
+  -e "s|std::string strBox = \"[^\"]*\";|std::string strBox = std::string(refshim_dir()) + \"/r\";|" \
+  -e "s|^\(\s*\)// Generate psiq for substrate gradient penalty|\1refshim_load_ic(psi_local.data(), alloc_local);|"
+
+# adv/cosAdvConSingle.cpp (conserved dynamics); argv = nu e0d radius N load
+DUMP='refshim_dump("psi", psi_local.data(), alloc_local); refshim_dump("vx", velx_local.data(), alloc_local); refshim_dump("vy", vely_local.data(), alloc_local); refshim_dump("vz", velz_local.data(), alloc_local); refshim_dump("gx", psiGradx_local.data(), alloc_local); refshim_dump("gy", psiGrady_local.data(), alloc_local); refshim_dump("gz", psiGradz_local.data(), alloc_local); refshim_dump("nq", Nq_local.data(), alloc_local);'
+build advc_ref adv/cosAdvConSingle.cpp \
+  -e "s/const ptrdiff_t Nx = atof(argv\[4\]), Ny = atof(argv\[4\]), Nz = atof(argv\[4\]);/const ptrdiff_t Nx = (ptrdiff_t)$P(\"NX\", 64), Ny = (ptrdiff_t)$P(\"NY\", 64), Nz = (ptrdiff_t)$P(\"NZ\", 64);/" \
+  -e "s/const double ep = -0.01\*ep_arg;/const double ep = $P(\"EPS\", -0.01*ep_arg);/" \
+  -e "s/double nu = atof(argv\[1\]);/double nu = $P(\"NU\", atof(argv[1]));/" \
+  -e "s|std::string strLoad = \"[^\"]*\";|std::string strLoad = std::string(refshim_dir()) + \"/r\";|" \
+  -e "s|std::string strBox = \"[^\"]*\";|std::string strBox = std::string(refshim_dir()) + \"/r\";|" \
+  -e "s|^\(\s*\)// Generate psiq for substrate gradient penalty|\1refshim_load_ic(psi_local.data(), alloc_local);|"

@@ -58,6 +58,7 @@ static void r3(orc_ctx *c, const double *in, double *out, int kx, int ky, int kz
 orc_ctx *orc_create(const orc_params *p)
 {
     if (p->nx < 2 || p->ny < 2 || p->nz < 2) return NULL;
+    if (p->conserved && p->model == ORC_QUASI) return NULL;   /* no conserved quasi in the reference */
     orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
     c->p = *p;
     c->nx = p->nx; c->ny = p->ny; c->nz = p->nz;
@@ -111,6 +112,19 @@ orc_ctx *orc_create(const orc_params *p)
                     c->aLin[idx] = p->eps - opSH;
                     c->C1[idx] = (2.0 - p->dt * c->rho_m * c->aLin[idx]);
                     c->C2[idx] = (1.5 - p->dt * c->rho_m * c->aLin[idx]);
+                } else if (p->conserved && p->model == ORC_NOADV) {
+                    /* q^2-weighted operator in aLin itself: no-adv/cosNoAdvConserv.cpp:646-650 */
+                    double opSH = p->alpha * pow(mq2 - q02, 2);
+                    c->aLin[idx] = mq2 * (p->eps - opSH);
+                    c->C1[idx] = (1.0 + dtd2 * c->aLin[idx]);
+                    c->C2[idx] = (1.0 - dtd2 * c->aLin[idx]);
+                } else if (p->conserved) {
+                    /* aLin stays L (it also builds Sp2); only C1, C2 carry q^2:
+                     * adv/cosAdvConSingle.cpp:738-742 */
+                    double opSH = p->alpha * pow(mq2 - q02, 2);
+                    c->aLin[idx] = p->eps - opSH;
+                    c->C1[idx] = (1.0 + dtd2 * mq2 * c->aLin[idx]);
+                    c->C2[idx] = (1.0 - dtd2 * mq2 * c->aLin[idx]);
                 } else {
                     double opSH = p->alpha * pow(mq2 - q02, 2);
                     c->aLin[idx] = p->eps - opSH;
@@ -180,6 +194,10 @@ int orc_set_psi(orc_ctx *c, const double *psi0)
          * adv/cosAdvTrackMult.cpp:760-777.  The wall potential has sigma = 0 (:75-82). */
         nonlin(c, c->psi, c->Nr);
         r3(c, c->Nr, c->Nq, T10, T10, T10);
+        /* conserved noadv weights the pre-loop N by q^2 (no-adv/cosNoAdvConserv.cpp:688-701);
+         * conserved adv keeps it unweighted (adv/cosAdvConSingle.cpp:762-780) */
+        if (c->p.conserved && c->p.model == ORC_NOADV)
+            for (long q = 0; q < n; q++) c->Nq[q] = c->mq2[q] * c->Nq[q];
         if (c->p.model == ORC_NOADV) {
             /* psiq is recomputed every step; keep the scaled transform for orc_get */
             r3(c, c->psi, c->psiq, T10, T10, T10);
@@ -321,6 +339,8 @@ static void step_noadv(orc_ctx *c)
     r3(c, c->Nr, c->Nq, T10, T10, T10);                            /* :727 */
     r3(c, c->psi, c->psiq, T10, T10, T10);                         /* :731 */
     if (c->surf_pending) surface_spectra(c, c->scale, c->scale);   /* :737-750 */
+    if (c->p.conserved)                                            /* cosNoAdvConserv.cpp:809 */
+        for (long q = 0; q < n; q++) c->Nq[q] = c->mq2[q] * c->Nq[q];
     for (long q = 0; q < n; q++)                                   /* :752-753 */
         c->psiq[q] = c->scale * (c->C1[q] * c->psiq[q] + dtd2 * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
     r3(c, c->psiq, c->psiNew, T01, T01, T01);                      /* :758 */
@@ -420,10 +440,22 @@ static void step_adv(orc_ctx *c)
     r3(c, c->vx, c->vx, S01, T01, T01);                             /* :1276-1286 */
     r3(c, c->vy, c->vy, T01, S01, T01);
     r3(c, c->vz, c->vz, T01, T01, S01);
-    for (long q = 0; q < n; q++)                                    /* :1290-1303 */
-        c->Nr[q] = b * pow(c->psi[q], 3) - g * pow(c->psi[q], 5) - c->vx[q] * c->gx[q] -
-                   c->vy[q] * c->gy[q] - c->vz[q] * c->gz[q];
-    r3(c, c->Nr, c->Nq, T10, T10, T10);                             /* :1307 */
+    if (c->p.conserved) {
+        /* conserved: N = q^2 CT(beta psi^3 - gamma psi^5) - CT(v . grad psi), the advection
+         * unweighted (adv/cosAdvConSingle.cpp:1296-1310,1369); Sx is free after stokes() */
+        for (long q = 0; q < n; q++) {
+            c->Nr[q] = b * pow(c->psi[q], 3) - g * pow(c->psi[q], 5);
+            c->Sx[q] = c->vx[q] * c->gx[q] + c->vy[q] * c->gy[q] + c->vz[q] * c->gz[q];
+        }
+        r3(c, c->Nr, c->Nq, T10, T10, T10);
+        r3(c, c->Sx, c->Sx, T10, T10, T10);
+        for (long q = 0; q < n; q++) c->Nq[q] = c->mq2[q] * c->Nq[q] - c->Sx[q];
+    } else {
+        for (long q = 0; q < n; q++)                                /* :1290-1303 */
+            c->Nr[q] = b * pow(c->psi[q], 3) - g * pow(c->psi[q], 5) - c->vx[q] * c->gx[q] -
+                       c->vy[q] * c->gy[q] - c->vz[q] * c->gz[q];
+        r3(c, c->Nr, c->Nq, T10, T10, T10);                         /* :1307 */
+    }
     if (c->surf_pending) surface_spectra(c, 1.0, c->scale);         /* :1311-1347 */
     for (long q = 0; q < n; q++)                                    /* :1355-1365 */
         c->psiq[q] = (c->C1[q] * c->psiq[q] + dtd2 * c->scale * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
@@ -546,7 +578,11 @@ int orc_step(orc_ctx *c, int nsteps)
 
 int orc_step_surface(orc_ctx *c, int *surf, double *vel, double *curvH, double *curvK)
 {
-    if (!c || !c->have_psi || c->p.model == ORC_QUASI || !surf || !vel || !curvH || !curvK) return -1;
+    /* conserved runs have no reference surface output to follow: adv/cosAdvConSingle.cpp
+     * comments it out (:1316-1352,1454-1524) and no-adv/cosNoAdvConserv.cpp evaluates its
+     * spectra from the updated, already scaled psihat with one more scale factor (:816-847) */
+    if (!c || !c->have_psi || c->p.model == ORC_QUASI || c->p.conserved || !surf || !vel || !curvH || !curvK)
+        return -1;
     c->s_idx = surf; c->s_vel = vel; c->s_H = curvH; c->s_K = curvK;
     c->surf_pending = 1;
     int rc = orc_step(c, 1);

@@ -33,6 +33,8 @@ typedef struct {
     double rho0, kp, amp; /* quasi density law: rho = kp sqrt(q0^2 psi^2 + |grad psi|^2) + rho0 */
     int divv_switch;    /* quasi: steps before div v comes from the mass balance (ref: 200) */
     int loaded;         /* quasi: the reference's load==1 branch semantics */
+    int conserved;      /* noadv, adv: conserved dynamics d psi/dt = -q^2 (dF/dpsi)^,
+                         * no-adv/cosNoAdvConserv.cpp, adv/cosAdvConSingle.cpp */
 } orc_params;
 
 typedef struct orc_ctx orc_ctx;

@@ -220,37 +220,80 @@ struct LdAdvN {
     }
 };
 
+// v . grad psi alone, the conserved adv model's unweighted advection term
+// (adv/cosAdvConSingle.cpp:1301-1303)
+template <typename T>
+struct LdAdvDot {
+    static constexpr int kMinBlocks = 2;   // six fields per point: memory-bound, keep registers
+    const T *__restrict__ vx, *__restrict__ vy, *__restrict__ vz;
+    const T *__restrict__ gx, *__restrict__ gy, *__restrict__ gz;
+    template <int V>
+    __device__ __forceinline__ void load(idx_t q, int, int, int, T *out) const
+    {
+        T a[V], b[V], c[V], d[V], e[V], f[V];
+        vld<T, V>(vx, q, a); vld<T, V>(gx, q, d);
+        vld<T, V>(vy, q, b); vld<T, V>(gy, q, e);
+        vld<T, V>(vz, q, c); vld<T, V>(gz, q, f);
+#pragma unroll
+        for (int u = 0; u < V; u++) out[u] = a[u] * d[u] + b[u] * e[u] + c[u] * f[u];
+    }
+};
+
 // ---------------------------------------------------------------- storers -------------
 // Crank-Nicolson / Adams-Bashforth update fed by the freshly transformed N
 // (no-adv/cosNoAdvTrackSing.cpp:752-753, adv/cosAdvTrackMult.cpp:1362-1364):
 //   psihat <- (C1 psihat + dt/2 scale (3 N - Nprev)) / C2,  C1,2 = 1 +- dt/2 L(q);  Nprev <- N
 // The update runs in FP64 from FP64 wavenumbers for every field precision: C1/C2 is applied
 // to psihat every step, so a rounding error in it would grow linearly with the step count.
-template <typename T>
+//
+// CONS selects the conserved variants (d psi/dt = -q^2 (dF/dpsi)^):
+//   1  noadv: the operator in C1, C2 and N are weighted by q^2
+//      (no-adv/cosNoAdvConserv.cpp:646-650,809);
+//   2  adv: C1, C2 and the Swift-Hohenberg part of N are weighted by q^2, the advection
+//      term is not: N = q^2 v - w with w = REDFT10^3(v . grad psi)
+//      (adv/cosAdvConSingle.cpp:741-742,1296-1310,1369).
+// Nprev keeps the weighted N, as the reference's NqPast does.
+template <typename T, int CONS = 0>
 struct StUpdCN {
     Spec<double> s;
     double *__restrict__ ph;        // spectral state (FP64 for every compute precision)
     T *__restrict__ np;             // Nprev (field precision)
-    static constexpr int PRE = 2;   // psihat, Nprev
+    const T *__restrict__ w = nullptr;   // CONS 2: REDFT10^3(v . grad psi)
+    // w is read ahead with psihat and Nprev for FP32 fields; FP64 fields read it in fin()
+    // (three FP64 reads ahead spill more at the FP64 passes' 128 registers)
+    static constexpr bool W_AHEAD = CONS == 2 && sizeof(T) == 4;
+    static constexpr int PRE = W_AHEAD ? 3 : 2;   // psihat, Nprev (, w)
     using Pre = double;
     template <int V>
     __device__ __forceinline__ void pre(idx_t q, int, int, int, double *buf) const
     {
         vld<double, V>(ph, q, buf);
         vld_as<double, V, T>(np, q, buf + V);
+        if constexpr (W_AHEAD) vld_as<double, V, T>(w, q, buf + 2 * V);
     }
     template <int V>
     __device__ __forceinline__ void fin(idx_t q, int i, int j, int k, const T *v, const double *buf) const
     {
         double o[V];
+        T nw[V], wl[V];
+        if constexpr (CONS == 2 && !W_AHEAD) vld<T, V>(w, q, wl);
 #pragma unroll
         for (int u = 0; u < V; u++) {
-            const double al = s.alin(i, j, k + u);
+            double al = s.alin(i, j, k + u);
+            double nn = double(v[u]);
+            if constexpr (CONS != 0) {
+                const double m2 = s.mq2(i, j, k + u);
+                al = m2 * al;
+                nn = m2 * nn;
+                if constexpr (W_AHEAD) nn -= buf[2 * V + u];
+                if constexpr (CONS == 2 && !W_AHEAD) nn -= double(wl[u]);
+            }
             const double c1 = 1.0 + s.dtd2 * al, c2 = 1.0 - s.dtd2 * al;
-            o[u] = (c1 * buf[u] + s.dtd2 * s.scale * (3.0 * double(v[u]) - buf[V + u])) / c2;
+            o[u] = (c1 * buf[u] + s.dtd2 * s.scale * (3.0 * nn - buf[V + u])) / c2;
+            nw[u] = T(nn);
         }
         vst<double, V>(ph, q, o);
-        vst<T, V>(np, q, v);
+        vst<T, V>(np, q, nw);
     }
     template <int V>
     __device__ __forceinline__ void store(idx_t q, int i, int j, int k, const T *v) const
@@ -258,6 +301,30 @@ struct StUpdCN {
         double buf[2 * V];
         pre<V>(q, i, j, k, buf);
         fin<V>(q, i, j, k, v, buf);
+    }
+};
+
+// q^2-weighted copy of a forward transform: the conserved noadv pre-loop N
+// (no-adv/cosNoAdvConserv.cpp:688-701)
+template <typename T>
+struct StQ2 {
+    Spec<double> s;
+    T *__restrict__ p;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(idx_t, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void fin(idx_t q, int i, int j, int k, const T *v, const T *) const
+    {
+        store<V>(q, i, j, k, v);
+    }
+    template <int V>
+    __device__ __forceinline__ void store(idx_t q, int i, int j, int k, const T *v) const
+    {
+        T o[V];
+#pragma unroll
+        for (int u = 0; u < V; u++) o[u] = T(s.mq2(i, j, k + u) * double(v[u]));
+        vst<T, V>(p, q, o);
     }
 };
 

@@ -313,7 +313,7 @@ const char *smadft_error_string(int code)
     case SMADFT_ERR_NOMEM: return "out of memory";
     case SMADFT_ERR_NONFINITE: return "non-finite field";
     case SMADFT_ERR_TIMEOUT: return "device wait timed out";
-    case SMADFT_ERR_UNSUPPORTED: return "unsupported grid length";
+    case SMADFT_ERR_UNSUPPORTED: return "unsupported grid length or model feature";
     case SMADFT_ERR_IO: return "checkpoint I/O error";
     case SMADFT_ERR_STATE: return "call out of order";
     case SMADFT_ERR_NODEVICE: return "no CUDA device";
@@ -350,6 +350,8 @@ int smadft_params_check(const smadft_params *p)
     if (!(p->nw > 0) || !(p->dt > 0) || !(p->q0 > 0)) return SMADFT_ERR_INVALID;
     if (p->model != SMADFT_MODEL_NOADV && !(p->nu > 0)) return SMADFT_ERR_INVALID;
     if (p->model == SMADFT_MODEL_QUASI && !(p->rho0 > 0)) return SMADFT_ERR_INVALID;
+    // the reference has conserved variants of noadv and adv only
+    if (p->conserved != 0 && (p->conserved != 1 || p->model == SMADFT_MODEL_QUASI)) return SMADFT_ERR_INVALID;
     return SMADFT_OK;
 }
 
@@ -571,6 +573,7 @@ int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH
     Ctx &c = h->c;
     if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
     if (c.p.model == SMADFT_MODEL_QUASI) return fail(c, SMADFT_ERR_UNSUPPORTED, "surface diagnostics: noadv and adv");
+    if (c.p.conserved) return fail(c, SMADFT_ERR_UNSUPPORTED, "surface diagnostics: non-conserved runs only");
     cudaSetDevice(c.dev);
     SurfaceScratch &sc = h->surf;
     const size_t cols = (size_t)c.g.nx * c.g.ny;
@@ -606,7 +609,8 @@ int smadft_adjoint(smadft_ctx *h, const smadft_adj_opts *o, smadft_grads *out, d
         return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if (!c.have_psi || c.steps != 0) return fail(c, SMADFT_ERR_STATE, "adjoint: start from the initial condition");
-    if (c.p.model != SMADFT_MODEL_NOADV) return fail(c, SMADFT_ERR_UNSUPPORTED, "adjoint: noadv only");
+    if (c.p.model != SMADFT_MODEL_NOADV || c.p.conserved)
+        return fail(c, SMADFT_ERR_UNSUPPORTED, "adjoint: non-conserved noadv only");
     cudaSetDevice(c.dev);
     std::memset(out, 0, sizeof(*out));
     int rc = c.f32 ? noadv_adjoint<float>(c, *o, out, d_psi0) : noadv_adjoint<double>(c, *o, out, d_psi0);

@@ -47,6 +47,14 @@ int adv_step(Ctx &c)
                                     LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr})))
             return rc;
     }
+    if (c.p.conserved) {
+        // conserved: N = q^2 REDFT10^3(beta psi^3 - gamma psi^5) - REDFT10^3(v.grad psi)
+        // (adv/cosAdvConSingle.cpp:1296-1310,1369); Sx is free once the velocity is out
+        if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdAdvDot<T>{vx, vy, vz, gx, gy, gz}, StoreArr<T>{Sx})))
+            return rc;
+        return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
+                        StUpdCN<T, 2>{make_spec<double>(c), ph, np, Sx});
+    }
     // N = beta psi^3 - gamma psi^5 - v.grad psi, CN/AB2 update (:1290-1365)
     return r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
                     LdAdvN<T>{psi, vx, vy, vz, gx, gy, gz, s.beta, s.gamma}, StUpdCN<T>{make_spec<double>(c), ph, np});

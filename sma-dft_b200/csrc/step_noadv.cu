@@ -12,9 +12,12 @@ int noadv_step(Ctx &c, bool keep_old)
     T *psi = c.f<T>(S_PSI);
     double *ph = c.f<double>(S_PSIH);   // spectral state (FP64)
     T *np = c.f<T>(S_NP);
-    // N^n = REDFT10^3(beta psi^3 - gamma psi^5), fused CN/AB2 update of psihat
-    int rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
-                      StUpdCN<T>{make_spec<double>(c), ph, np});
+    // N^n = REDFT10^3(beta psi^3 - gamma psi^5), fused CN/AB2 update of psihat (q^2-weighted
+    // operator and N for conserved runs)
+    int rc = c.p.conserved ? r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
+                                      StUpdCN<T, 1>{make_spec<double>(c), ph, np})
+                           : r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma},
+                                      StUpdCN<T>{make_spec<double>(c), ph, np});
     if (rc) return rc;
     // psi^{n+1} = REDFT01^3 psihat (into the second buffer when the old psi is needed)
     T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
@@ -37,9 +40,15 @@ int pre_loop(Ctx &c)
     int rc;
     if (c.p.model == SMADFT_MODEL_QUASI) return quasi_pre_loop<T>(c);
     // psihat = scale REDFT10^3 psi ; Nprev = REDFT10^3(beta psi^3 - gamma psi^5) (no advection)
-    // no-adv/cosNoAdvTrackSing.cpp:618-635, adv/cosAdvTrackMult.cpp:760-777
+    // no-adv/cosNoAdvTrackSing.cpp:618-635, adv/cosAdvTrackMult.cpp:760-777; weighted by q^2
+    // for conserved noadv (no-adv/cosNoAdvConserv.cpp:688-701), unweighted for conserved adv
+    // (adv/cosAdvConSingle.cpp:762-780)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{psi}, StScale<T>{ph, c.scale}))) return rc;
-    if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma}, StoreArr<T>{np}))) return rc;
+    if (c.p.conserved && c.p.model == SMADFT_MODEL_NOADV)
+        rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma}, StQ2<T>{make_spec<double>(c), np});
+    else
+        rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdNonlin<T>{psi, s.beta, s.gamma}, StoreArr<T>{np});
+    if (rc) return rc;
     return SMADFT_OK;
 }
 

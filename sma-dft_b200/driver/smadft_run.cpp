@@ -9,8 +9,11 @@
 //
 // usage: smadft_run noadv|adv|quasi [nu e0d radius load] [key=value ...]
 //   keys: n nx ny nz nw dt eps alpha beta gamma nu kp rho0 divv steps l1every saveevery
-//         precision(fp64|fp32) ic(interface|bump|focal|conics|file:<path>) A radius seed
-//         noise out track_axis track_mode track_hi track_lo checkpoint resume
+//         precision(fp64|fp32) conserved(0|1) ic(interface|bump|focal|conics|file:<path>) A
+//         radius seed noise out track_axis track_mode track_hi track_lo checkpoint resume
+// conserved=1 runs the reference's conserved variants (no-adv/cosNoAdvConserv.cpp,
+// adv/cosAdvConSingle.cpp); their save iteration writes surfPsi.dat but no velSurf/curvH/curvK
+// values (the library has no conserved surface diagnostics).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -93,6 +96,7 @@ int main(int argc, char **argv)
     p.nu = o.num("nu", p.nu); p.kp = o.num("kp", p.kp); p.rho0 = o.num("rho0", p.rho0);
     p.divv_switch = (int)o.num("divv", p.divv_switch);
     p.precision = o.get("precision", "fp64") == "fp32" ? SMADFT_FP32 : SMADFT_FP64;
+    p.conserved = (int)o.num("conserved", 0);
     const long steps = (long)o.num("steps", 1000);
     const int l1every = (int)o.num("l1every", m == SMADFT_MODEL_QUASI ? 50 : 100);
     const int saveevery = (int)o.num("saveevery", 10);
@@ -141,7 +145,8 @@ int main(int argc, char **argv)
         info << "Nx: " << p.nx << "\nNy: " << p.ny << "\nNz: " << p.nz << "\nPoints per wavelength (nw): "
              << p.nw << "\nq0 (z direction): " << p.q0 << "\nepsilon: " << p.eps << "\nbeta: " << p.beta
              << "\ngamma: " << p.gamma << "\nViscosity (nu): " << p.nu << "\ndt: " << p.dt
-             << "\nprecision: " << (p.precision == SMADFT_FP32 ? "fp32" : "fp64") << "\n";
+             << "\nprecision: " << (p.precision == SMADFT_FP32 ? "fp32" : "fp64")
+             << "\nconserved: " << p.conserved << "\n";
     }
     long done = 0;
     int countSave = 0;
@@ -152,7 +157,7 @@ int main(int argc, char **argv)
     // the reference's own save iteration (z-scanning flat tracker, noadv / adv) also writes the
     // normal velocity and curvatures of that step (no-adv/cosNoAdvTrackSing.cpp:808-1021,
     // adv/cosAdvTrackMult.cpp:1311-1585)
-    const bool with_surface = m != SMADFT_MODEL_QUASI && taxis == 2 && tmode == SMADFT_TRACK_FLAT;
+    const bool with_surface = m != SMADFT_MODEL_QUASI && !p.conserved && taxis == 2 && tmode == SMADFT_TRACK_FLAT;
     while (done < steps) {
         long chunk = std::min<long>(l1every - 1, steps - done - 1);
         if (chunk > 0 && (rc = smadft_step(ctx, (int)chunk))) return die("smadft_step", rc, ctx);

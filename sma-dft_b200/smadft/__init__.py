@@ -46,7 +46,7 @@ class Params(ctypes.Structure):
         ("eps", ctypes.c_double), ("q0", ctypes.c_double), ("nu", ctypes.c_double),
         ("rho0", ctypes.c_double), ("kp", ctypes.c_double), ("amp", ctypes.c_double),
         ("divv_switch", ctypes.c_int), ("loaded", ctypes.c_int), ("device", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("conserved", ctypes.c_int), ("reserved", ctypes.c_int * 4),
     ]
 
 

@@ -2,11 +2,12 @@
 
 The reference has no tests or golden files of its own, so the vectors here come from the
 reference loop bodies themselves: oracle/build_ref.sh compiles no-adv/cosNoAdvTrackSing.cpp,
-no-adv/cosNoAdvTrackBump.cpp, adv/cosAdvTrackMult.cpp and quasi/quasi.cpp with a single-rank
+no-adv/cosNoAdvTrackBump.cpp, no-adv/cosNoAdvConserv.cpp, adv/cosAdvTrackMult.cpp,
+adv/cosAdvConSingle.cpp and quasi/quasi.cpp with a single-rank
 MPI shim and an FFTW-r2r shim (oracle/r2r.c), and this script runs them on small seeded
 grids, recording the initial condition, the final fields and the text diagnostics.
 
-    python tests/golden/make_golden.py        # needs oracle/_ref/ (run oracle/build_ref.sh)
+    python tests/golden/make_golden.py [name ...]   # needs oracle/_ref/ (run oracle/build_ref.sh)
 
 Each case is (model, shape, steps, IC amplitude, interface normal, parameters).  The shapes are deliberately not cubic so
 that axis mix-ups show.
@@ -34,6 +35,10 @@ CASES = {
     "quasi_16x12x20_s60_kp": ("quasi", (16, 12, 20), 60, 1.328, 0,
                               dict(nw=8, dt=0.002, eps=-0.75, nu=1.0, kp=0.3755, rho0=1.0, divv=20)),
     "bump_16x12x32_s1000": ("bump", (16, 12, 32), 1000, 1.328, 2, dict(nw=8, dt=0.05, eps=-0.7)),
+    # conserved dynamics (no-adv/cosNoAdvConserv.cpp, adv/cosAdvConSingle.cpp): the q^2-weighted
+    # explicit term needs a smaller step than the non-conserved runs at nw = 8
+    "noadvc_16x12x20_s200": ("noadvc", (16, 12, 20), 200, 1.328, 0, dict(nw=8, dt=0.005, eps=-0.75)),
+    "advc_16x12x20_s100": ("advc", (16, 12, 20), 100, 1.328, 0, dict(nw=8, dt=0.005, eps=-0.75, nu=1.0)),
 }
 
 
@@ -84,9 +89,9 @@ def make(name: str) -> str:
 
 
 def main():
-    if not all(oracle.reference_available(w) for w in ("noadv", "bump", "adv", "quasi")):
+    if not all(oracle.reference_available(w) for w in oracle.REF_BINARIES):
         raise SystemExit("oracle/_ref is not built: run oracle/build_ref.sh first")
-    for name in CASES:
+    for name in sys.argv[1:] or CASES:
         p = make(name)
         print("wrote", p, os.path.getsize(p), "bytes")
 

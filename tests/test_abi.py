@@ -65,6 +65,17 @@ def test_quasi_and_adv_need_positive_viscosity(smadft_lib):
     assert smadft_lib.smadft_params_check(ctypes.byref(p)) == 0
 
 
+def test_conserved_flag_only_for_noadv_and_adv(smadft_lib):
+    for model in (smadft.NOADV, smadft.ADV):
+        p = smadft.params(model, (16, 16, 16), conserved=1)
+        assert smadft_lib.smadft_params_check(ctypes.byref(p)) == 0
+        p.conserved = 2
+        assert smadft_lib.smadft_params_check(ctypes.byref(p)) == -1
+    p = smadft.params(smadft.QUASI, (16, 16, 16), conserved=1)
+    assert smadft_lib.smadft_params_check(ctypes.byref(p)) == -1
+    assert ctypes.sizeof(smadft.Params) == 144       # the flag took a reserved slot
+
+
 def test_error_strings(smadft_lib):
     assert smadft_lib.smadft_error_string(-4) == b"non-finite field"
     assert smadft_lib.smadft_abi_version() == 1

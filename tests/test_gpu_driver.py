@@ -64,3 +64,35 @@ def test_driver_outputs_match_oracle(tmp_path, model, omodel, extra):
         assert np.max(np.abs(got[found] - w[found])) <= 1e-9 * np.max(np.abs(w[found])), name
     final = read(tmp_path / "psi0.dat").reshape(shape)
     assert np.max(np.abs(final - o.get(oracle.F_PSI))) <= 1e-10 * np.max(np.abs(final))
+
+
+@pytest.mark.parametrize("model,omodel,extra", [
+    ("noadv", oracle.NOADV, dict(dt=0.005)),
+    ("adv", oracle.ADV, dict(dt=0.005, nu=1.0)),
+])
+def test_driver_conserved_run_matches_oracle(tmp_path, model, omodel, extra):
+    if not os.path.exists(DRIVER):
+        pytest.skip("smadft_run not built")
+    shape = (16, 12, 20)
+    z = np.arange(shape[2]) * 2 * np.pi / 8
+    rng = np.random.default_rng(12)
+    psi0 = 1.3 * np.cos(z)[None, None, :] * np.ones((shape[0], shape[1], 1)) + 0.01 * rng.standard_normal(shape)
+    ic = tmp_path / "ic.txt"
+    np.savetxt(ic, psi0.reshape(-1), fmt="%.17g")
+    args = [DRIVER, model, f"nx={shape[0]}", f"ny={shape[1]}", f"nz={shape[2]}", "nw=8", "eps=-0.7",
+            "conserved=1", "steps=20", "l1every=10", "saveevery=2", f"ic=file:{ic}", f"out={tmp_path}"]
+    args += [f"{k}={v}" for k, v in extra.items()]
+    subprocess.run(args, check=True, capture_output=True, text=True)
+
+    o = oracle.Oracle(omodel, shape, nw=8, eps=-0.7, conserved=1, **extra)
+    o.set_psi(psi0)
+    o.step(10)
+    l1_10 = o.diag()["l1"]
+    o.step(10)
+    l1_20 = o.diag()["l1"]
+    assert np.allclose(read(tmp_path / "L1.dat"), [l1_10, l1_20], rtol=1e-10, atol=0)
+    idx, _ = o.track(axis=2, mode=0, hi=0.7, lo=0.0)
+    assert np.array_equal(read(tmp_path / "surfPsi.dat"), idx.reshape(-1).astype(float))
+    assert read(tmp_path / "velSurf.dat").size == 0      # no conserved surface diagnostics
+    final = read(tmp_path / "psi0.dat").reshape(shape)
+    assert np.max(np.abs(final - o.get(oracle.F_PSI))) <= 1e-10 * np.max(np.abs(final))

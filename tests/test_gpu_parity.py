@@ -15,7 +15,9 @@ import smadft
 pytestmark = pytest.mark.gpu
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
-MODEL = {"noadv": smadft.NOADV, "bump": smadft.NOADV, "adv": smadft.ADV, "quasi": smadft.QUASI}
+MODEL = {"noadv": smadft.NOADV, "bump": smadft.NOADV, "adv": smadft.ADV, "quasi": smadft.QUASI,
+         "noadvc": smadft.NOADV, "advc": smadft.ADV}
+CONSERVED = {"noadvc", "advc"}
 OMODEL = {smadft.NOADV: oracle.NOADV, smadft.ADV: oracle.ADV, smadft.QUASI: oracle.QUASI}
 GFIELD = {"psi": "psi", "nq": "nhat", "vx": "vx", "vy": "vy", "vz": "vz", "gx": "gx", "gy": "gy",
           "gz": "gz", "rho": "rho", "p": "p", "mu": "mu", "energy": "energy", "psiq": "psihat"}
@@ -32,7 +34,8 @@ def rel_l2(a, b):
 def solver_for(which, shape, params, precision=smadft.FP64):
     kw = dict(params)
     divv = int(kw.pop("divv", 200))
-    p = smadft.params(MODEL[which], shape, precision=precision, divv_switch=divv, **kw)
+    p = smadft.params(MODEL[which], shape, precision=precision, divv_switch=divv,
+                      conserved=int(which in CONSERVED), **kw)
     return smadft.Solver(p)
 
 

@@ -15,7 +15,9 @@ import pytest
 import oracle
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
-MODEL = {"noadv": oracle.NOADV, "bump": oracle.NOADV, "adv": oracle.ADV, "quasi": oracle.QUASI}
+MODEL = {"noadv": oracle.NOADV, "bump": oracle.NOADV, "adv": oracle.ADV, "quasi": oracle.QUASI,
+         "noadvc": oracle.NOADV, "advc": oracle.ADV}
+CONSERVED = {"noadvc", "advc"}
 FIELD = {"psi": oracle.F_PSI, "nq": oracle.F_NHAT, "vx": oracle.F_VX, "vy": oracle.F_VY,
          "vz": oracle.F_VZ, "gx": oracle.F_GX, "gy": oracle.F_GY, "gz": oracle.F_GZ,
          "rho": oracle.F_RHO, "p": oracle.F_P, "mu": oracle.F_MU, "energy": oracle.F_ENERGY,
@@ -32,11 +34,11 @@ def golden_case(path):
 def oracle_for(which, shape, params):
     kw = dict(params)
     divv = int(kw.pop("divv", 200))
-    return oracle.Oracle(MODEL[which], shape, divv_switch=divv, **kw)
+    return oracle.Oracle(MODEL[which], shape, divv_switch=divv, conserved=int(which in CONSERVED), **kw)
 
 
 def test_golden_files_present():
-    assert len(GOLDEN) >= 7
+    assert len(GOLDEN) >= 9
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
@@ -78,7 +80,7 @@ def test_oracle_matches_golden(path):
         assert np.array_equal(idx[found].astype(float), d["t_surfPsi"][found])
 
 
-needs_ref = pytest.mark.skipif(not all(oracle.reference_available(w) for w in ("noadv", "adv", "quasi")),
+needs_ref = pytest.mark.skipif(not all(oracle.reference_available(w) for w in oracle.REF_BINARIES),
                                reason="oracle/_ref not built (oracle/build_ref.sh)")
 
 
@@ -87,6 +89,8 @@ needs_ref = pytest.mark.skipif(not all(oracle.reference_available(w) for w in ("
     ("noadv", (12, 10, 8), 7, dict(nw=8, dt=0.05, eps=-0.7)),
     ("adv", (10, 8, 12), 5, dict(nw=8, dt=0.02, eps=-0.7, nu=2.0)),
     ("quasi", (8, 12, 10), 6, dict(nw=8, dt=0.002, eps=-0.7, nu=1.0, kp=0.3, rho0=1.0, divv=2)),
+    ("noadvc", (12, 10, 8), 30, dict(nw=8, dt=0.005, eps=-0.7)),
+    ("advc", (10, 8, 12), 20, dict(nw=8, dt=0.005, eps=-0.7, nu=2.0)),
 ])
 def test_oracle_matches_live_reference(which, shape, steps, params):
     rng = np.random.default_rng(99)
