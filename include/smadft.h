@@ -229,10 +229,11 @@ int smadft_batch_step(smadft_batch *batch, int nsteps);
 int smadft_batch_sync(smadft_batch *batch);
 const char *smadft_batch_last_error(const smadft_batch *batch);
 
-/* ---- adjoint (diffusive model) ---------------------------------------------------------
- * Gradients of an interface loss with respect to eps, alpha, beta, gamma and the initial
- * psi, by a hand-written adjoint of the semi-implicit step (transposed transforms,
- * linearised nonlinearity; the reference has no counterpart).  The run must be at its
+/* ---- adjoint (diffusive and advected models) -------------------------------------------
+ * Gradients of an interface loss with respect to eps, alpha, beta, gamma (adv: and nu) and
+ * the initial psi, by a hand-written adjoint of the semi-implicit step (transposed
+ * transforms, linearised nonlinearity, transposed Stokes projection; the reference has no
+ * counterpart).  The run must be at its
  * initial condition (right after smadft_set_psi).  smadft_adjoint advances it `steps`
  * loop bodies, keeping psihat and the AB2 history every `checkpoint_every` steps, takes
  * loss = mean sub-grid interface position (in lambda0) over the columns the tracker
@@ -240,8 +241,8 @@ const char *smadft_batch_last_error(const smadft_batch *batch);
  * final psi, then runs the reverse sweep, re-running each segment from its checkpoint.  The
  * found set and crossing cells are held fixed (as a small central difference sees them).
  * d_psi0 (may be NULL) receives dloss/dpsi_0 (nx*ny*nz doubles).  The run continues from
- * the final state.  Non-conserved noadv only (SMADFT_ERR_UNSUPPORTED otherwise).
- * Synchronises. */
+ * the final state.  Non-conserved noadv and adv (SMADFT_ERR_UNSUPPORTED for quasi and
+ * conserved runs).  Synchronises. */
 typedef struct {
     int steps;              /* loop bodies                                   */
     int checkpoint_every;   /* K: psihat / Nhat_prev kept every K steps       */
@@ -252,6 +253,7 @@ typedef struct {
     double loss;            /* mean interface position, lambda0 units        */
     int found;              /* columns in the loss                           */
     double d_eps, d_alpha, d_beta, d_gamma;
+    double d_nu;            /* adv: dloss/dnu (noadv: 0)                      */
 } smadft_grads;
 int smadft_adjoint(smadft_ctx *ctx, const smadft_adj_opts *opts, smadft_grads *out, double *d_psi0);
 

@@ -609,14 +609,18 @@ int smadft_adjoint(smadft_ctx *h, const smadft_adj_opts *o, smadft_grads *out, d
         return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if (!c.have_psi || c.steps != 0) return fail(c, SMADFT_ERR_STATE, "adjoint: start from the initial condition");
-    if (c.p.model != SMADFT_MODEL_NOADV || c.p.conserved)
-        return fail(c, SMADFT_ERR_UNSUPPORTED, "adjoint: non-conserved noadv only");
+    if (c.p.model == SMADFT_MODEL_QUASI || c.p.conserved)
+        return fail(c, SMADFT_ERR_UNSUPPORTED, "adjoint: non-conserved noadv and adv only");
     cudaSetDevice(c.dev);
     std::memset(out, 0, sizeof(*out));
-    int rc = c.f32 ? noadv_adjoint<float>(c, *o, out, d_psi0) : noadv_adjoint<double>(c, *o, out, d_psi0);
+    int rc;
+    if (c.p.model == SMADFT_MODEL_ADV)
+        rc = c.f32 ? adv_adjoint<float>(c, *o, out, d_psi0) : adv_adjoint<double>(c, *o, out, d_psi0);
+    else
+        rc = c.f32 ? noadv_adjoint<float>(c, *o, out, d_psi0) : noadv_adjoint<double>(c, *o, out, d_psi0);
     if (rc) return rc;
     c.steps += o->steps;
-    c.psi_current = true;
+    c.psi_current = c.p.model != SMADFT_MODEL_ADV;   // adv: S_PSI holds psi of the last step's start
     return SMADFT_OK;
 }
 

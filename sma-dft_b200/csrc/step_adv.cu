@@ -4,13 +4,14 @@
 
 namespace smadft {
 
+// psi, grad psi, Sp2, the force spectra S-hat and the velocity v of the current psihat: the
+// loop body up to N (adv/cosAdvTrackMult.cpp:847-1286)
 template <typename T>
-int adv_step(Ctx &c)
+int adv_fields(Ctx &c)
 {
     Spec<T> s = make_spec<T>(c);
     T *psi = c.f<T>(S_PSI);
     double *ph = c.f<double>(S_PSIH);   // spectral state (FP64)
-    T *np = c.f<T>(S_NP);
     T *gx = c.f<T>(S_GX), *gy = c.f<T>(S_GY), *gz = c.f<T>(S_GZ), *sp2 = c.f<T>(S_SP2);
     T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
     T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
@@ -47,6 +48,21 @@ int adv_step(Ctx &c)
                                     LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr})))
             return rc;
     }
+    return SMADFT_OK;
+}
+
+template <typename T>
+int adv_step(Ctx &c)
+{
+    int rc = adv_fields<T>(c);
+    if (rc) return rc;
+    Spec<T> s = make_spec<T>(c);
+    T *psi = c.f<T>(S_PSI);
+    double *ph = c.f<double>(S_PSIH);
+    T *np = c.f<T>(S_NP);
+    T *gx = c.f<T>(S_GX), *gy = c.f<T>(S_GY), *gz = c.f<T>(S_GZ);
+    T *Sx = c.f<T>(S_SX);
+    T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
     if (c.p.conserved) {
         // conserved: N = q^2 REDFT10^3(beta psi^3 - gamma psi^5) - REDFT10^3(v.grad psi)
         // (adv/cosAdvConSingle.cpp:1296-1310,1369); Sx is free once the velocity is out
@@ -63,9 +79,11 @@ int adv_step(Ctx &c)
 // each precision builds as its own object (SMADFT_INST_FLOAT / SMADFT_INST_DOUBLE); a plain
 // compile without either instantiates both
 #if !defined(SMADFT_INST_DOUBLE)
+template int adv_fields<float>(Ctx &);
 template int adv_step<float>(Ctx &);
 #endif
 #if !defined(SMADFT_INST_FLOAT)
+template int adv_fields<double>(Ctx &);
 template int adv_step<double>(Ctx &);
 #endif
 

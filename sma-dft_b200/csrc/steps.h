@@ -10,6 +10,8 @@ namespace smadft {
 template <typename T> int noadv_step(Ctx &c, bool keep_old);
 // adv/cosAdvTrackMult.cpp:824-1369,1742
 template <typename T> int adv_step(Ctx &c);
+// its first part (:847-1286): psi, grad psi, Sp2, S-hat and v from psihat into their slots
+template <typename T> int adv_fields(Ctx &c);
 // quasi/quasi.cpp:1099-2190 (nloop = 1-based step counter)
 template <typename T> int quasi_step(Ctx &c, long long nloop, bool keep_old);
 // pre-loop blocks: no-adv :618-635, adv :760-777, quasi :990-1062
@@ -37,5 +39,7 @@ struct SurfaceScratch {
 template <typename T> int surface_step(Ctx &c, SurfaceScratch &sc);
 // adjoint of `o.steps` noadv loop bodies from the initial condition (adjoint.cu)
 template <typename T> int noadv_adjoint(Ctx &c, const smadft_adj_opts &o, smadft_grads *out, double *dpsi0_host);
+// the same for the advected model (adjoint.cu)
+template <typename T> int adv_adjoint(Ctx &c, const smadft_adj_opts &o, smadft_grads *out, double *dpsi0_host);
 
 }  // namespace smadft

@@ -70,7 +70,8 @@ class AdjOpts(ctypes.Structure):
 class Grads(ctypes.Structure):
     """smadft_grads"""
     _fields_ = [("loss", ctypes.c_double), ("found", ctypes.c_int), ("d_eps", ctypes.c_double),
-                ("d_alpha", ctypes.c_double), ("d_beta", ctypes.c_double), ("d_gamma", ctypes.c_double)]
+                ("d_alpha", ctypes.c_double), ("d_beta", ctypes.c_double), ("d_gamma", ctypes.c_double),
+                ("d_nu", ctypes.c_double)]
 
 
 class TuneReport(ctypes.Structure):
@@ -312,14 +313,15 @@ class Solver:
 
     def adjoint(self, steps: int, checkpoint_every: int = 50, axis: int = 0, mode: int = TRACK_BUMP,
                 hi: float = 0.6, lo: float = 0.1, want_dpsi0: bool = True) -> dict:
-        """Interface-loss gradients of `steps` noadv loop bodies from the initial condition."""
+        """Interface-loss gradients of `steps` noadv or adv loop bodies from the initial
+        condition (nu: adv only, 0 for noadv)."""
         o = AdjOpts(int(steps), int(checkpoint_every), int(axis), int(mode), float(hi), float(lo))
         g = Grads()
         dpsi = np.empty(self.shape, dtype=np.float64) if want_dpsi0 else None
         _check(lib().smadft_adjoint(self._h, ctypes.byref(o), ctypes.byref(g),
                                     _dptr(dpsi) if dpsi is not None else None), self._h)
         return dict(loss=g.loss, found=g.found, eps=g.d_eps, alpha=g.d_alpha, beta=g.d_beta, gamma=g.d_gamma,
-                    psi0=dpsi)
+                    nu=g.d_nu, psi0=dpsi)
 
     def autotune(self, steps: int = 5) -> dict:
         """Time each applicable kernel path on this run and keep the fastest (state kept)."""

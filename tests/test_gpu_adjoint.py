@@ -100,7 +100,7 @@ def test_fp32_adjoint_matches_fp64_adjoint(adj64):
     assert rel <= 1e-3
 
 
-def test_adjoint_needs_initial_state_and_noadv():
+def test_adjoint_needs_initial_state_and_a_supported_model():
     psi0 = psi_init()
     with smadft.Solver(make()) as s:
         s.set_psi(psi0)
@@ -108,7 +108,7 @@ def test_adjoint_needs_initial_state_and_noadv():
         with pytest.raises(smadft.SmadftError) as e:
             s.adjoint(5, checkpoint_every=5, **TRACK)
         assert e.value.code == -8
-    p = smadft.params(smadft.ADV, (16, 16, 16))
+    p = smadft.params(smadft.QUASI, (16, 16, 16))
     with smadft.Solver(p) as s:
         s.set_psi(np.zeros((16, 16, 16)))
         with pytest.raises(smadft.SmadftError) as e:
