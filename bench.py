@@ -324,6 +324,68 @@ def run_batch_sweep(torch, smadft, steps, rank, world, dist):
     return out
 
 
+def run_adjoint_c5(torch, smadft, steps):
+    """Config 5: the adjoint of the adv step at 128^3, dt = 0.02, checkpoints every 50 steps
+    over `steps` steps, FP32 forward + adjoint, with the FP64 adjoint and a central
+    difference of the FP64 forward (eps and nu) beside it.  The loss is the mean tracked
+    interface position (bump tracker along x), so the initial condition is the x-normal
+    interface with a bump (config 3's focal-conic field has no interface).  Times are host
+    wall clock around one smadft_adjoint call (which synchronises), allocations included."""
+    n, K = 128, 50
+    kw = dict(CFG)
+    kw["dt"] = 0.02
+    track = dict(axis=0, mode=smadft.TRACK_BUMP, hi=0.6, lo=0.1)
+    psi0 = smadft.ic_interface(smadft.params(smadft.ADV, (n, n, n), **kw), A=1.328, bump=0.5 * 2 * np.pi,
+                               noise=1e-3, seed=20240601)
+    out = {"config": f"adv {n}^3, dt=0.02, {steps} steps, checkpoints every {K}; interface IC (x-normal, bump); "
+                     "loss = mean bump-tracked interface position (lambda0)"}
+    grads = {}
+    for prec, name in ((smadft.FP32, "fp32"), (smadft.FP64, "fp64")):
+        p = smadft.params(smadft.ADV, (n, n, n), precision=prec, **kw)
+        with smadft.Solver(p) as s:
+            s.set_psi(psi0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g = s.adjoint(steps, checkpoint_every=K, **track)
+            out[f"adjoint_{name}_ms"] = 1000.0 * (time.perf_counter() - t0)
+        with smadft.Solver(p) as s:
+            s.set_psi(psi0)
+            s.step(3)
+            s.sync()
+            t0 = time.perf_counter()
+            s.step(steps)
+            s.sync()
+            out[f"forward_{name}_ms"] = 1000.0 * (time.perf_counter() - t0)
+        grads[name] = g
+    names = ("eps", "alpha", "beta", "gamma", "nu")
+    out["grad_fp32"] = {k: grads["fp32"][k] for k in names}
+    out["grad_fp64"] = {k: grads["fp64"][k] for k in names}
+    out["found_columns"] = grads["fp64"]["found"]
+    out["max_rel_err_fp32_vs_fp64"] = max(abs(grads["fp32"][k] - grads["fp64"][k]) / abs(grads["fp64"][k])
+                                          for k in names)
+    d32, d64 = grads["fp32"]["psi0"], grads["fp64"]["psi0"]
+    out["psi0_rel_l2_fp32_vs_fp64"] = float(np.linalg.norm(d32 - d64) / np.linalg.norm(d64))
+
+    def loss(**over):
+        kk = dict(kw)
+        kk.update(over)
+        with smadft.Solver(smadft.params(smadft.ADV, (n, n, n), **kk)) as s:
+            s.set_psi(psi0)
+            s.step(steps)
+            idx, pos = s.track(**track)
+        m = (idx >= 0) & np.isfinite(pos)
+        return pos[m].mean() / kk["nw"], int(m.sum())
+    h = 1e-7
+    fd = {}
+    for k in ("eps", "nu"):
+        jp, fp = loss(**{k: kw[k] + h})
+        jm, fm = loss(**{k: kw[k] - h})
+        fd[k] = {"fd": (jp - jm) / (2 * h), "same_found_set": fp == fm == grads["fp64"]["found"],
+                 "rel_err_fp64_adjoint": abs(grads["fp64"][k] - (jp - jm) / (2 * h)) / abs((jp - jm) / (2 * h))}
+    out["central_difference_h1e-7"] = fd
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import smadft
@@ -410,6 +472,7 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    adjoint = run_adjoint_c5(torch, smadft, args.adjoint_steps) if args.adjoint_steps > 0 else None
 
     algo_bytes = 4.0 * N ** 3 * F_ADV
     achieved_step = algo_bytes / (ms_step * 1e-3) / 1e9
@@ -450,6 +513,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 8 * N ** 3},
         "gpu_launches": launches_fp32,
         "batch_sweep": sweep,
+        "adjoint": adjoint,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
@@ -506,6 +570,8 @@ def main():
     ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "r2r3d", "step"], default=None,
                     help="launch one kernel family a few times (for profilers) and exit")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--adjoint-steps", type=int, default=500,
+                    help="steps of the 128^3 adv adjoint measurement (0: skip)")
     ap.add_argument("--shape", type=int, default=N)
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
