@@ -23,9 +23,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
-NOADV, ADV, QUASI = 0, 1, 2
+NOADV, ADV, QUASI, COMP = 0, 1, 2, 3
 F_PSI, F_PSIHAT, F_VX, F_VY, F_VZ, F_GX, F_GY, F_GZ = range(8)
 F_RHO, F_P, F_DIVV, F_MU, F_ENERGY, F_NHAT = range(8, 14)
+F_AMP, F_VSOLX, F_VSOLY, F_VSOLZ, F_VIRRX, F_VIRRY, F_VIRRZ, F_FRHO = range(14, 22)
 REDFT10, REDFT01, RODFT10, RODFT01 = 0, 1, 2, 3
 
 
@@ -40,6 +41,7 @@ class OrcParams(ctypes.Structure):
         ("rho0", ctypes.c_double), ("kp", ctypes.c_double), ("amp", ctypes.c_double),
         ("divv_switch", ctypes.c_int), ("loaded", ctypes.c_int),
         ("conserved", ctypes.c_int),
+        ("zeta", ctypes.c_double), ("rho_up", ctypes.c_int),
     ]
 
 
@@ -108,7 +110,8 @@ def r2r_3d(x, kinds) -> np.ndarray:
 
 
 DEFAULTS = dict(nw=8.0, dt=0.05, alpha=1.0, beta=2.0, gamma=1.0, eps=-0.75, q0=1.0, nu=1.0,
-                rho0=1.0, kp=0.0, amp=1.34164, divv_switch=200, loaded=0, conserved=0)
+                rho0=1.0, kp=0.0, amp=1.34164, divv_switch=200, loaded=0, conserved=0,
+                zeta=0.001, rho_up=16)
 
 
 class Oracle:
@@ -118,8 +121,9 @@ class Oracle:
         p = dict(DEFAULTS)
         p.update(kw)
         self.shape = tuple(int(s) for s in shape)
-        self.params = OrcParams(model=int(model), nx=self.shape[0], ny=self.shape[1],
-                                nz=self.shape[2], **{k: p[k] for k in DEFAULTS})
+        ints = {name for name, t in OrcParams._fields_ if t is ctypes.c_int}
+        self.params = OrcParams(model=int(model), nx=self.shape[0], ny=self.shape[1], nz=self.shape[2],
+                                **{k: (int(p[k]) if k in ints else p[k]) for k in DEFAULTS})
         self._c = lib().orc_create(ctypes.byref(self.params))
         if not self._c:
             raise ValueError("orc_create rejected the parameters")
@@ -178,11 +182,13 @@ class Oracle:
 # The reference itself, compiled from its sources by build_ref.sh (single-rank shims).
 # ----------------------------------------------------------------------------------
 REF_BINARIES = {"noadv": "noadv_ref", "bump": "bump_ref", "adv": "adv_ref", "quasi": "quasi_ref",
-                "noadvc": "noadvc_ref", "advc": "advc_ref"}
+                "noadvc": "noadvc_ref", "advc": "advc_ref", "comp": "comp_ref"}
 REF_DUMPS = {
     "noadv": ["psi", "nq"],
     "noadvc": ["psi", "nq"],
     "advc": ["psi", "vx", "vy", "vz", "gx", "gy", "gz", "nq"],
+    "comp": ["psi", "rho", "psiq", "amp", "divv", "mu", "vsolx", "vsoly", "vsolz", "virrx", "virry", "virrz",
+             "nl", "frho"],
     "bump": ["psi"],
     "adv": ["psi", "vx", "vy", "vz", "gx", "gy", "gz", "nq"],
     "quasi": ["psi", "rho", "p", "vx", "vy", "vz", "mu", "energy", "psiq"],
@@ -228,6 +234,8 @@ def run_reference(which: str, shape, steps: int, psi0=None, workdir: str | None 
         elif which == "quasi":
             argv += ["1", "75", "10", "0"]
             os.makedirs(os.path.join(wd, "r1-e0d75"), exist_ok=True)
+        elif which == "comp":
+            argv += ["1", "75", "10", "0"]          # nu e0d radius load
         elif which == "noadvc":
             argv += ["75", "10", str(nx), "0"]      # e0d radius N load
             os.makedirs(os.path.join(wd, "r75-r10"), exist_ok=True)

@@ -13,7 +13,7 @@
 #   * psiMid's hard-coded j = 256 (noadv Sing)        -> Ny/2 (in range for small grids)
 #   * L1/mass/energy/velSurf/curvH/curvK text output  -> 17 significant digits
 #   * before MPI::Finalize(), binary dumps of the final fields
-# Usage: oracle/build_ref.sh   (writes oracle/_ref/{noadv,bump,adv,quasi,noadvc,advc}_ref)
+# Usage: oracle/build_ref.sh   (writes oracle/_ref/{noadv,bump,adv,quasi,noadvc,advc,comp}_ref)
 set -euo pipefail
 REF="${SMADFT_REFERENCE:-/root/reference}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
@@ -110,3 +110,19 @@ build advc_ref adv/cosAdvConSingle.cpp \
   -e "s|std::string strLoad = \"[^\"]*\";|std::string strLoad = std::string(refshim_dir()) + \"/r\";|" \
   -e "s|std::string strBox = \"[^\"]*\";|std::string strBox = std::string(refshim_dir()) + \"/r\";|" \
   -e "s|^\(\s*\)// Generate psiq for substrate gradient penalty|\1refshim_load_ic(psi_local.data(), alloc_local);|"
+
+# compressible/compressible.cpp (independent density, amplitude field); argv = nu e0d radius load
+DUMP='refshim_dump("psi", psi_local.data(), alloc_local); refshim_dump("rho", rho_local.data(), alloc_local); refshim_dump("psiq", psiq_local.data(), alloc_local); refshim_dump("amp", amp_local.data(), alloc_local); refshim_dump("divv", divv_local.data(), alloc_local); refshim_dump("mu", mu_local.data(), alloc_local); refshim_dump("vsolx", vsolx_local.data(), alloc_local); refshim_dump("vsoly", vsoly_local.data(), alloc_local); refshim_dump("vsolz", vsolz_local.data(), alloc_local); refshim_dump("virrx", virrx_local.data(), alloc_local); refshim_dump("virry", virry_local.data(), alloc_local); refshim_dump("virrz", virrz_local.data(), alloc_local); refshim_dump("nl", Nl_local.data(), alloc_local); refshim_dump("frho", f_rho_local.data(), alloc_local);'
+build comp_ref compressible/compressible.cpp \
+  -e "s/const double ep = -0.001\*ep_arg;/const double ep = $P(\"EPS\", -0.001*ep_arg);/" \
+  -e "s/double nu = atof(argv\[1\]);/double nu = $P(\"NU\", atof(argv[1]));/" \
+  -e "s/double rho_0 = \([0-9.]*\);/double rho_0 = $P(\"RHO0\", \1);/" \
+  -e "s/double zeta = \([0-9.]*\);/double zeta = $P(\"ZETA\", \1);/" \
+  -e "s/const int divvSwitch = \([0-9]*\);/const int divvSwitch = (int)$P(\"DIVV\", \1);/" \
+  -e "s/const int rhoUP = \([0-9]*\);/const int rhoUP = (int)$P(\"RHO_UP\", \1);/" \
+  -e "s|std::string strLoad = \"[^\"]*\";|std::string strLoad = std::string(refshim_dir()) + \"/\";|" \
+  -e "s|std::string strSave = \"[^\"]*\";|std::string strSave = std::string(refshim_dir()) + \"/\";|" \
+  -e "s|std::string strBox = \"[^\"]*\";|std::string strBox = std::string(refshim_dir()) + \"/\";|" \
+  -e "s|mass_output << rho_sum << |mass_output << std::setprecision(17) << rho_sum << |" \
+  -e "s|energy_output << energy << |energy_output << std::setprecision(17) << energy << |" \
+  -e "s|^\(\s*\)/\*\* Create output files \*\*/|\1refshim_load_ic(psi_local.data(), alloc_local);|"

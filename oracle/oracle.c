@@ -31,6 +31,9 @@ struct orc_ctx {
     /* quasi */
     double *psiq_old, *psi_old, *rho, *rhoq, *rho_old, *p_, *divv, *mu, *energy, *dfd, *lap;
     double *rdx, *rdy, *rdz;
+    /* compressible */
+    double *amp, *fgrad, *ampd, *frho, *virx, *viry, *virz, *fxs, *fys, *fzs;
+    double amp_c, kp_c;         /* compressible/compressible.cpp:265-267 */
     /* surface diagnostics of one step (orc_step_surface) */
     int surf_pending;
     double *dTpsi, *psiDxx, *psiDyy, *psiDzz, *fgx, *fgy, *fgz;
@@ -58,7 +61,7 @@ static void r3(orc_ctx *c, const double *in, double *out, int kx, int ky, int kz
 orc_ctx *orc_create(const orc_params *p)
 {
     if (p->nx < 2 || p->ny < 2 || p->nz < 2) return NULL;
-    if (p->conserved && p->model == ORC_QUASI) return NULL;   /* no conserved quasi in the reference */
+    if (p->conserved && (p->model == ORC_QUASI || p->model == ORC_COMP)) return NULL;   /* none in the reference */
     orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
     c->p = *p;
     c->nx = p->nx; c->ny = p->ny; c->nz = p->nz;
@@ -73,6 +76,15 @@ orc_ctx *orc_create(const orc_params *p)
     double rho_s = p->kp * p->amp + p->rho0;
     c->rho_m = rho_s / 2;
     c->lambda = -2 * p->nu / 3;
+    if (p->model == ORC_COMP) {
+        /* compressible/compressible.cpp:265-271: Amp of the one-mode smectic at eps, kp such
+         * that rho_s = kp Amp + rho_0 = 1, rho_m = rho_s / 2, lambda = nu */
+        c->amp_c = sqrt((3 * p->beta + sqrt(9 * p->beta * p->beta + 40 * p->eps * p->gamma)) / 5);
+        c->kp_c = (1 - p->rho0) / c->amp_c;
+        rho_s = c->kp_c * c->amp_c + p->rho0;
+        c->rho_m = rho_s / 2;
+        c->lambda = p->nu;
+    }
     /* wavenumbers: no-adv/cosNoAdvTrackSing.cpp:309-324 (DCT), adv/cosAdvTrackMult.cpp:386-401 (DST) */
     c->qx = dal(c->nx); c->sx = dal(c->nx);
     c->qy = dal(c->ny); c->sy = dal(c->ny);
@@ -90,7 +102,12 @@ orc_ctx *orc_create(const orc_params *p)
         c->Sx = dal(n); c->Sy = dal(n); c->Sz = dal(n);
         c->vx = dal(n); c->vy = dal(n); c->vz = dal(n);
     }
-    if (p->model == ORC_QUASI) {
+    if (p->model == ORC_COMP) {
+        c->amp = dal(n); c->fgrad = dal(n); c->ampd = dal(n); c->frho = dal(n);
+        c->virx = dal(n); c->viry = dal(n); c->virz = dal(n);
+        c->fxs = dal(n); c->fys = dal(n); c->fzs = dal(n);
+    }
+    if (p->model == ORC_QUASI || p->model == ORC_COMP) {
         c->psiq_old = dal(n); c->psi_old = dal(n); c->rho = dal(n); c->rhoq = dal(n);
         c->rho_old = dal(n); c->p_ = dal(n); c->divv = dal(n); c->mu = dal(n); c->energy = dal(n);
         c->dfd = dal(n); c->lap = dal(n); c->rdx = dal(n); c->rdy = dal(n); c->rdz = dal(n);
@@ -107,7 +124,7 @@ orc_ctx *orc_create(const orc_params *p)
                 double mq2 = pow(c->qx[i], 2) + pow(c->qy[j], 2) + pow(c->qz[k], 2);
                 c->mq2[idx] = mq2;
                 double q02 = p->q0 * p->q0;
-                if (p->model == ORC_QUASI) {
+                if (p->model == ORC_QUASI || p->model == ORC_COMP) {
                     double opSH = p->alpha * pow(q02 - mq2, 2);
                     c->aLin[idx] = p->eps - opSH;
                     c->C1[idx] = (2.0 - p->dt * c->rho_m * c->aLin[idx]);
@@ -131,7 +148,18 @@ orc_ctx *orc_create(const orc_params *p)
                     c->C1[idx] = (1.0 + dtd2 * c->aLin[idx]);
                     c->C2[idx] = (1.0 - dtd2 * c->aLin[idx]);
                 }
-                if (p->model != ORC_NOADV) {
+                if (p->model == ORC_COMP) {
+                    /* compressible/compressible.cpp:1092-1100: CM1 = scale/|q_s|^2 (nu applied later) */
+                    double m2 = pow(c->sx[i], 2) + pow(c->qy[j], 2) + pow(c->qz[k], 2);
+                    c->CM1x[idx] = c->scale / (m2);
+                    c->CM2x[idx] = c->sx[i] / m2;
+                    m2 = pow(c->qx[i], 2) + pow(c->sy[j], 2) + pow(c->qz[k], 2);
+                    c->CM1y[idx] = c->scale / (m2);
+                    c->CM2y[idx] = c->sy[j] / m2;
+                    m2 = pow(c->qx[i], 2) + pow(c->qy[j], 2) + pow(c->sz[k], 2);
+                    c->CM1z[idx] = c->scale / (m2);
+                    c->CM2z[idx] = c->sz[k] / m2;
+                } else if (p->model != ORC_NOADV) {
                     double m2 = pow(c->sx[i], 2) + pow(c->qy[j], 2) + pow(c->qz[k], 2);
                     c->CM1x[idx] = c->scale / (p->nu * m2);
                     c->CM2x[idx] = c->sx[i] / m2;
@@ -154,7 +182,9 @@ void orc_destroy(orc_ctx *c)
                        &c->psi, &c->psiq, &c->psiNew, &c->Nr, &c->Nq, &c->NqPast, &c->gx, &c->gy,
                        &c->gz, &c->sp2, &c->Sx, &c->Sy, &c->Sz, &c->vx, &c->vy, &c->vz,
                        &c->psiq_old, &c->psi_old, &c->rho, &c->rhoq, &c->rho_old, &c->p_,
-                       &c->divv, &c->mu, &c->energy, &c->dfd, &c->lap, &c->rdx, &c->rdy, &c->rdz};
+                       &c->divv, &c->mu, &c->energy, &c->dfd, &c->lap, &c->rdx, &c->rdy, &c->rdz,
+                       &c->amp, &c->fgrad, &c->ampd, &c->frho, &c->virx, &c->viry, &c->virz,
+                       &c->fxs, &c->fys, &c->fzs};
     for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); q++) free(*ptrs[q]);
     free(c->dTpsi); free(c->psiDxx); free(c->psiDyy); free(c->psiDzz);
     free(c->fgx); free(c->fgy); free(c->fgz);
@@ -174,7 +204,20 @@ int orc_set_psi(orc_ctx *c, const double *psi0)
     memcpy(c->psi, psi0, sizeof(double) * n);
     c->nloop = 0;
     c->L1 = c->mass = c->en = 0.0;
-    if (c->p.model == ORC_QUASI) {
+    if (c->p.model == ORC_COMP) {
+        /* compressible/compressible.cpp:1104-1135: psiq = s CT(psi), psi = iCT(psiq), N^0
+         * (unused: the first step sets Nl_old = Nl), psiq_old, psi_old; rho and its rate start
+         * at zero (load != 1, :579-580) */
+        r3(c, c->psi, c->psiq, T10, T10, T10);
+        for (long q = 0; q < n; q++) c->psiq[q] = c->scale * c->psiq[q];
+        r3(c, c->psiq, c->psi, T01, T01, T01);
+        nonlin(c, c->psi, c->Nr);
+        memcpy(c->psiq_old, c->psiq, sizeof(double) * n);
+        r3(c, c->Nr, c->Nq, T10, T10, T10);
+        memcpy(c->psi_old, c->psi, sizeof(double) * n);
+        memset(c->rho, 0, sizeof(double) * n);
+        memset(c->frho, 0, sizeof(double) * n);
+    } else if (c->p.model == ORC_QUASI) {
         /* quasi/quasi.cpp:990-1034: psiq = scale CT(psi), psi = iCT(psiq), N^0, psiq_old, psi_old */
         r3(c, c->psi, c->psiq, T10, T10, T10);
         for (long q = 0; q < n; q++) c->psiq[q] = c->scale * c->psiq[q];
@@ -565,12 +608,210 @@ static void step_quasi(orc_ctx *c)
     c->en = es * c->dx * c->dx * c->dx;
 }
 
+/* ---------------- compressible: compressible/compressible.cpp:1265-2720 ----------------
+ * Single-rank semantics: the halo planes read as zero, so the last x-plane of the shifted
+ * spectra and of v_x stay zero and the i = 0 neighbours of the y, z velocities and of the
+ * divergence are zero.  Each expression keeps the reference's operand order. */
+static void step_comp(orc_ctx *c)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const long n = c->n, nyz = (long)ny * nz;
+    const orc_params *P = &c->p;
+    const double scale = c->scale, dt = P->dt, dtd2 = P->dt / 2;
+    const double beta = P->beta, gamma = P->gamma, alpha = P->alpha, ep = P->eps;
+    const double q02 = P->q0 * P->q0, nu = P->nu, lambda = c->lambda, zeta = P->zeta;
+    const double rho_0 = P->rho0, kp = c->kp_c, Amp = c->amp_c;
+    c->nloop++;                                                      /* :1268 */
+    const long nLoop = c->nloop;
+    memcpy(c->NqPast, c->Nq, sizeof(double) * n);                    /* :1283 Nl_old = Nl */
+    r3(c, c->rho, c->rhoq, T10, T10, T10);                           /* :1287-1289 */
+    /* shifted gradient spectra of psi and rho (:1290-1388) */
+    memset(c->gx, 0, sizeof(double) * n); memset(c->gy, 0, sizeof(double) * n); memset(c->gz, 0, sizeof(double) * n);
+    memset(c->rdx, 0, sizeof(double) * n); memset(c->rdy, 0, sizeof(double) * n); memset(c->rdz, 0, sizeof(double) * n);
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                const long q = IDX(c, i, j, k);
+                if (i < nx - 1) {
+                    c->gx[q] = -c->sx[i] * c->psiq[q + nyz];
+                    c->rdx[q] = -scale * c->sx[i] * c->rhoq[q + nyz];
+                }
+                if (j < ny - 1) {
+                    c->gy[q] = -c->sy[j] * c->psiq[q + nz];
+                    c->rdy[q] = -scale * c->sy[j] * c->rhoq[q + nz];
+                }
+                if (k < nz - 1) {
+                    c->gz[q] = -c->sz[k] * c->psiq[q + 1];
+                    c->rdz[q] = -scale * c->sz[k] * c->rhoq[q + 1];
+                }
+            }
+    r3(c, c->gx, c->gx, S01, T01, T01);                              /* :1390-1408 */
+    r3(c, c->gy, c->gy, T01, S01, T01);
+    r3(c, c->gz, c->gz, T01, T01, S01);
+    r3(c, c->rdx, c->rdx, S01, T01, T01);
+    r3(c, c->rdy, c->rdy, T01, S01, T01);
+    r3(c, c->rdz, c->rdz, T01, T01, S01);
+    /* amplitude, Gaussian-filtered (:1420-1456) */
+    for (long q = 0; q < n; q++)
+        c->amp[q] = sqrt(q02 * pow(c->psi[q], 2) + pow(c->gx[q], 2) + pow(c->gy[q], 2) + pow(c->gz[q], 2));
+    r3(c, c->amp, c->amp, T10, T10, T10);
+    for (long q = 0; q < n; q++) c->amp[q] = scale * c->amp[q] * exp(-1.57 * 1.57 * c->mq2[q] * 2);
+    r3(c, c->amp, c->amp, T01, T01, T01);
+    /* dF/d(lap psi) (:1460-1474) */
+    for (long q = 0; q < n; q++) c->dfd[q] = alpha * (q02 - c->mq2[q]) * c->psiq[q];
+    r3(c, c->dfd, c->dfd, T01, T01, T01);
+    /* lap(rho dF/dlap psi) (:1478-1560): after the relaxation steps rho is independent;
+     * during them rho follows the amplitude, shifted up by rho_up planes */
+    if (nLoop > P->divv_switch || P->loaded) {
+        for (long q = 0; q < n; q++) c->lap[q] = c->rho[q] * c->dfd[q];
+        r3(c, c->lap, c->lap, T10, T10, T10);
+        for (long q = 0; q < n; q++) c->lap[q] = -scale * c->mq2[q] * c->lap[q];
+        r3(c, c->lap, c->lap, T01, T01, T01);
+    } else {
+        for (long q = 0; q < n; q++) c->lap[q] = -c->mq2[q] * alpha * (q02 - c->mq2[q]) * c->psiq[q];
+        r3(c, c->lap, c->lap, T01, T01, T01);
+        for (long q = 0; q < n; q++) {
+            const double rho_1 = rho_0;
+            c->rho[q] = rho_1 + ((1 - rho_1) / Amp) * c->amp[q];
+            c->lap[q] = c->rho[q] * c->lap[q];
+        }
+        if (P->rho_up > 0) {
+            const int up = P->rho_up;
+            for (int i = 0; i < nx; i++)
+                for (int j = 0; j < ny; j++) {
+                    const long col = IDX(c, i, j, 0);
+                    for (int k = nz - 1; k > up - 1; k--) {
+                        c->rho[col + k] = c->rho[col + k - up];
+                        c->lap[col + k] = c->rho[col + k] * c->lap[col + k];
+                    }
+                    for (int k = 0; k < up && k < nz; k++) {
+                        c->rho[col + k] = 1;
+                        c->lap[col + k] = c->rho[col + k] * c->lap[col + k];
+                    }
+                }
+        }
+    }
+    /* forces, chemical potential, density penalty (:1564-1610) */
+    for (long q = 0; q < n; q++) {
+        c->energy[q] = 0.5 * pow(c->dfd[q], 2);
+        c->fgrad[q] = 0.5 * zeta * (pow(c->rho[q], 2) - pow(rho_0 + kp * c->amp[q], 2));
+        c->mu[q] = c->lap[q] + c->rho[q] * (c->dfd[q]);
+        c->Sx[q] = c->mu[q] * c->gx[q] + c->energy[q] * c->rdx[q];
+        c->Sy[q] = c->mu[q] * c->gy[q] + c->energy[q] * c->rdy[q];
+        c->Sz[q] = c->mu[q] * c->gz[q] + c->energy[q] * c->rdz[q];
+        c->mu[q] = c->lap[q] + c->rho[q] * (c->dfd[q] - ep * c->psi[q] - beta * pow(c->psi[q], 3) +
+                                            gamma * pow(c->psi[q], 5));
+        c->energy[q] = c->rho[q] * c->energy[q];
+        const double fx = kp * zeta * (c->rho[q] - rho_0 - kp * c->amp[q]) / (c->amp[q] + 0.001);
+        c->fxs[q] = fx * c->gx[q];
+        c->fys[q] = fx * c->gy[q];
+        c->fzs[q] = fx * c->gz[q];
+    }
+    r3(c, c->fgrad, c->fgrad, T10, T10, T10);                        /* :1614-1700 */
+    r3(c, c->energy, c->energy, T10, T10, T10);
+    r3(c, c->Sx, c->Sx, S10, T10, T10);
+    r3(c, c->Sy, c->Sy, T10, S10, T10);
+    r3(c, c->Sz, c->Sz, T10, T10, S10);
+    r3(c, c->fxs, c->fxs, S10, T10, T10);
+    r3(c, c->fys, c->fys, T10, S10, T10);
+    r3(c, c->fzs, c->fzs, T10, T10, S10);
+    for (long q = 0; q < n; q++) c->fgrad[q] = c->fgrad[q] + c->energy[q] * exp(-1.57 * 1.57 * c->mq2[q] * 2); /* :1826-1835 */
+    /* solenoidal and irrotational velocity spectra (:1838-2410) */
+    memset(c->vx, 0, sizeof(double) * n); memset(c->vy, 0, sizeof(double) * n); memset(c->vz, 0, sizeof(double) * n);
+    memset(c->virx, 0, sizeof(double) * n); memset(c->viry, 0, sizeof(double) * n); memset(c->virz, 0, sizeof(double) * n);
+    const double l2n = lambda + 2 * nu;
+    for (int i = 0; i < nx - 1; i++)                                 /* :1966-2085 */
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                const long q = IDX(c, i, j, k);
+                const double Sy = (j != 0) ? c->Sy[IDX(c, i + 1, j - 1, k)] : 0.0;
+                const double Sz = (k != 0) ? c->Sz[IDX(c, i + 1, j, k - 1)] : 0.0;
+                const double dot = c->sx[i] * c->Sx[q] + c->qy[j] * Sy + c->qz[k] * Sz;
+                c->vx[q] = (c->CM1x[q] / nu) * (c->Sx[q] - c->CM2x[q] * dot);
+                c->virx[q] = (c->CM1x[q] / l2n) *
+                             (c->sx[i] * c->fgrad[q + nyz] + c->CM2x[q] * dot * exp(-1.57 * 1.57 * 2 * scale / c->CM1x[q]));
+            }
+    for (int i = 0; i < nx; i++)                                     /* :2135-2410 */
+        for (int j = 0; j < ny - 1; j++)
+            for (int k = 0; k < nz - 1; k++) {
+                const long q = IDX(c, i, j, k);
+                double Sx = (i != 0) ? c->Sx[IDX(c, i - 1, j + 1, k)] : 0.0;
+                const double Sz = (k != 0) ? c->Sz[IDX(c, i, j + 1, k - 1)] : 0.0;
+                double dot = c->qx[i] * Sx + c->sy[j] * c->Sy[q] + c->qz[k] * Sz;
+                c->vy[q] = (c->CM1y[q] / nu) * (c->Sy[q] - c->CM2y[q] * dot);
+                c->viry[q] = (c->CM1y[q] / l2n) *
+                             (c->sy[j] * c->fgrad[q + nz] + c->CM2y[q] * dot * exp(-1.57 * 1.57 * 2 * scale / c->CM1y[q]));
+                Sx = (i != 0) ? c->Sx[IDX(c, i - 1, j, k + 1)] : 0.0;
+                const double Sy = (j != 0) ? c->Sy[IDX(c, i, j - 1, k + 1)] : 0.0;
+                dot = c->qx[i] * Sx + c->qy[j] * Sy + c->sz[k] * c->Sz[q];
+                c->vz[q] = (c->CM1z[q] / nu) * (c->Sz[q] - c->CM2z[q] * dot);
+                /* the k = 0 branch for i >= 1, 0 < j < ny-1 filters with CM1y (:2348-2350) */
+                const double cmf = (i >= 1 && k == 0 && j >= 1) ? c->CM1y[q] : c->CM1z[q];
+                c->virz[q] = (c->CM1z[q] / l2n) *
+                             (c->sz[k] * c->fgrad[q + 1] + c->CM2z[q] * dot * exp(-1.57 * 1.57 * 2 * scale / cmf));
+            }
+    /* divergence of the irrotational part and the penalty force term (:2478-2527) */
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                const long q = IDX(c, i, j, k);
+                const double Sx = i > 0 ? c->virx[q - nyz] : 0.0, fx = i > 0 ? c->fxs[q - nyz] : 0.0;
+                const double Sy = j > 0 ? c->viry[q - nz] : 0.0, fy = j > 0 ? c->fys[q - nz] : 0.0;
+                const double Sz = k > 0 ? c->virz[q - 1] : 0.0, fz = k > 0 ? c->fzs[q - 1] : 0.0;
+                c->divv[q] = c->qx[i] * Sx + c->qy[j] * Sy + c->qz[k] * Sz;
+                c->ampd[q] = scale * (c->qx[i] * fx + c->qy[j] * fy + c->qz[k] * fz);
+            }
+    r3(c, c->divv, c->divv, T01, T01, T01);
+    r3(c, c->ampd, c->ampd, T01, T01, T01);
+    r3(c, c->vx, c->vx, S01, T01, T01);                              /* :2529-2552 */
+    r3(c, c->vy, c->vy, T01, S01, T01);
+    r3(c, c->vz, c->vz, T01, T01, S01);
+    r3(c, c->virx, c->virx, S01, T01, T01);
+    r3(c, c->viry, c->viry, T01, S01, T01);
+    r3(c, c->virz, c->virz, T01, T01, S01);
+    /* mass balance, AB2 in real space (:2556-2572) */
+    for (long q = 0; q < n; q++) {
+        const double S = -(c->vx[q] + c->virx[q]) * c->rdx[q] - (c->vy[q] + c->viry[q]) * c->rdy[q] -
+                         (c->vz[q] + c->virz[q]) * c->rdz[q] - c->rho[q] * c->divv[q];
+        c->rho[q] = c->rho[q] + dt * (1.5 * S - 0.5 * c->frho[q]);
+        c->frho[q] = S;
+    }
+    /* N (:2576-2596) */
+    for (long q = 0; q < n; q++)
+        c->Nr[q] = -c->mu[q] + (kp * zeta / (c->amp[q] + 0.001)) * (c->rho[q] - rho_0 - kp * c->amp[q]) * c->psi[q] -
+                   c->ampd[q] - (c->vx[q] + c->virx[q]) * c->gx[q] - (c->vy[q] + c->viry[q]) * c->gy[q] -
+                   (c->vz[q] + c->virz[q]) * c->gz[q];
+    r3(c, c->Nr, c->Nq, T10, T10, T10);                              /* :2600-2602 */
+    if (nLoop == 1) memcpy(c->NqPast, c->Nq, sizeof(double) * n);    /* :2604-2606 */
+    for (long q = 0; q < n; q++) {                                   /* :2618-2629 */
+        const double old = c->psiq[q];
+        c->psiq[q] = (c->C1[q] * c->psiq[q] - 0.5 * c->psiq_old[q] +
+                      dtd2 * scale * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
+        c->psiq_old[q] = old;
+    }
+    memcpy(c->psi_old, c->psi, sizeof(double) * n);                  /* :2633 */
+    r3(c, c->psiq, c->psi, T01, T01, T01);                           /* :2635-2637 */
+    /* diagnostics (:2642-2690), every step here */
+    c->L1 = l1_measure(c, c->psi, c->psi_old);
+    double rs = 0.0, es = 0.0;
+    for (long q = 0; q < n; q++) {
+        rs = rs + c->rho[q];
+        const double e = -0.5 * ep * pow(c->psi[q], 2) + 0.5 * pow(c->dfd[q], 2) - 0.25 * beta * pow(c->psi[q], 4) +
+                         (gamma / 6) * pow(c->psi[q], 6);
+        c->energy[q] = e;
+        es = es + c->rho[q] * e + 0.5 * zeta * pow(c->rho[q] - rho_0 - kp * c->amp[q], 2);
+    }
+    c->mass = rs * c->dx * c->dx * c->dx;
+    c->en = es * c->dx * c->dx * c->dx;
+}
+
 int orc_step(orc_ctx *c, int nsteps)
 {
     if (!c || !c->have_psi) return -1;
     for (int s = 0; s < nsteps; s++) {
         if (c->p.model == ORC_NOADV) { step_noadv(c); c->nloop++; }
         else if (c->p.model == ORC_ADV) { step_adv(c); c->nloop++; }
+        else if (c->p.model == ORC_COMP) step_comp(c);
         else step_quasi(c);
     }
     return 0;
@@ -581,7 +822,7 @@ int orc_step_surface(orc_ctx *c, int *surf, double *vel, double *curvH, double *
     /* conserved runs have no reference surface output to follow: adv/cosAdvConSingle.cpp
      * comments it out (:1316-1352,1454-1524) and no-adv/cosNoAdvConserv.cpp evaluates its
      * spectra from the updated, already scaled psihat with one more scale factor (:816-847) */
-    if (!c || !c->have_psi || c->p.model == ORC_QUASI || c->p.conserved || !surf || !vel || !curvH || !curvK)
+    if (!c || !c->have_psi || c->p.model >= ORC_QUASI || c->p.conserved || !surf || !vel || !curvH || !curvK)
         return -1;
     c->s_idx = surf; c->s_vel = vel; c->s_H = curvH; c->s_K = curvK;
     c->surf_pending = 1;
@@ -609,6 +850,14 @@ int orc_get(const orc_ctx *c, int field, double *out)
     case ORC_F_MU: src = c->mu; break;
     case ORC_F_ENERGY: src = c->energy; break;
     case ORC_F_NHAT: src = c->Nq; break;
+    case ORC_F_AMP: src = c->amp; break;
+    case ORC_F_VSOLX: src = c->p.model == ORC_COMP ? c->vx : NULL; break;
+    case ORC_F_VSOLY: src = c->p.model == ORC_COMP ? c->vy : NULL; break;
+    case ORC_F_VSOLZ: src = c->p.model == ORC_COMP ? c->vz : NULL; break;
+    case ORC_F_VIRRX: src = c->virx; break;
+    case ORC_F_VIRRY: src = c->viry; break;
+    case ORC_F_VIRRZ: src = c->virz; break;
+    case ORC_F_FRHO: src = c->frho; break;
     default: return -1;
     }
     if (!src) return -1;

@@ -8,6 +8,7 @@
  *   ORC_NOADV  no-adv/cosNoAdvTrackSing.cpp:584-1074   (diffusive, CN/AB2)
  *   ORC_ADV    adv/cosAdvTrackMult.cpp:717-1744          (advected, Stokes projection)
  *   ORC_QUASI  quasi/quasi.cpp:951-2498                  (quasi-incompressible, BDF2-like)
+ *   ORC_COMP   compressible/compressible.cpp:1079-2720   (independent density, amplitude field)
  *
  * Parity is pinned two ways (tests/test_oracle_pin.py): against the reference's own
  * sources compiled here with a single-rank MPI shim and an FFTW-r2r shim (oracle/_ref,
@@ -21,7 +22,7 @@
 extern "C" {
 #endif
 
-enum { ORC_NOADV = 0, ORC_ADV = 1, ORC_QUASI = 2 };
+enum { ORC_NOADV = 0, ORC_ADV = 1, ORC_QUASI = 2, ORC_COMP = 3 };
 
 typedef struct {
     int model;
@@ -35,6 +36,8 @@ typedef struct {
     int loaded;         /* quasi: the reference's load==1 branch semantics */
     int conserved;      /* noadv, adv: conserved dynamics d psi/dt = -q^2 (dF/dpsi)^,
                          * no-adv/cosNoAdvConserv.cpp, adv/cosAdvConSingle.cpp */
+    double zeta;        /* comp: density penalty (ref 0.001); rho0 is the comp rho_0 (ref 0.01) */
+    int rho_up;         /* comp: z shift of rho in the relaxation steps (ref 16) */
 } orc_params;
 
 typedef struct orc_ctx orc_ctx;
@@ -48,7 +51,11 @@ enum {
     ORC_F_RHO = 8, ORC_F_P = 9, ORC_F_DIVV = 10,   /* quasi: filtered rho, pressure, div v (spectral) */
     ORC_F_MU = 11, ORC_F_ENERGY = 12,              /* quasi: chemical potential, energy density */
     ORC_F_NHAT = 13,                               /* unscaled REDFT10^3 of the nonlinear term */
-    ORC_F_COUNT = 14
+    ORC_F_AMP = 14,                                /* comp: filtered amplitude */
+    ORC_F_VSOLX = 15, ORC_F_VSOLY = 16, ORC_F_VSOLZ = 17,   /* comp: solenoidal velocity */
+    ORC_F_VIRRX = 18, ORC_F_VIRRY = 19, ORC_F_VIRRZ = 20,   /* comp: irrotational velocity */
+    ORC_F_FRHO = 21,                               /* comp: the density rate of the last step */
+    ORC_F_COUNT = 22
 };
 
 orc_ctx *orc_create(const orc_params *p);

@@ -3,7 +3,7 @@
 The reference has no tests or golden files of its own, so the vectors here come from the
 reference loop bodies themselves: oracle/build_ref.sh compiles no-adv/cosNoAdvTrackSing.cpp,
 no-adv/cosNoAdvTrackBump.cpp, no-adv/cosNoAdvConserv.cpp, adv/cosAdvTrackMult.cpp,
-adv/cosAdvConSingle.cpp and quasi/quasi.cpp with a single-rank
+adv/cosAdvConSingle.cpp, quasi/quasi.cpp and compressible/compressible.cpp with a single-rank
 MPI shim and an FFTW-r2r shim (oracle/r2r.c), and this script runs them on small seeded
 grids, recording the initial condition, the final fields and the text diagnostics.
 
@@ -39,6 +39,10 @@ CASES = {
     # explicit term needs a smaller step than the non-conserved runs at nw = 8
     "noadvc_16x12x20_s200": ("noadvc", (16, 12, 20), 200, 1.328, 0, dict(nw=8, dt=0.005, eps=-0.75)),
     "advc_16x12x20_s100": ("advc", (16, 12, 20), 100, 1.328, 0, dict(nw=8, dt=0.005, eps=-0.75, nu=1.0)),
+    # compressible/compressible.cpp: 40 relaxation steps (rho from the amplitude, shifted up
+    # by rho_up) then the independent density
+    "comp_16x12x20_s100": ("comp", (16, 12, 20), 100, 1.3, 0,
+                           dict(nw=8, dt=0.001, eps=-0.75, nu=1.0, rho0=0.01, zeta=0.001, rho_up=16, divv=40)),
 }
 
 

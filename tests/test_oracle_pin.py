@@ -16,12 +16,14 @@ import oracle
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 MODEL = {"noadv": oracle.NOADV, "bump": oracle.NOADV, "adv": oracle.ADV, "quasi": oracle.QUASI,
-         "noadvc": oracle.NOADV, "advc": oracle.ADV}
+         "noadvc": oracle.NOADV, "advc": oracle.ADV, "comp": oracle.COMP}
 CONSERVED = {"noadvc", "advc"}
 FIELD = {"psi": oracle.F_PSI, "nq": oracle.F_NHAT, "vx": oracle.F_VX, "vy": oracle.F_VY,
          "vz": oracle.F_VZ, "gx": oracle.F_GX, "gy": oracle.F_GY, "gz": oracle.F_GZ,
          "rho": oracle.F_RHO, "p": oracle.F_P, "mu": oracle.F_MU, "energy": oracle.F_ENERGY,
-         "psiq": oracle.F_PSIHAT}
+         "psiq": oracle.F_PSIHAT, "amp": oracle.F_AMP, "divv": oracle.F_DIVV, "vsolx": oracle.F_VSOLX,
+         "vsoly": oracle.F_VSOLY, "vsolz": oracle.F_VSOLZ, "virrx": oracle.F_VIRRX, "virry": oracle.F_VIRRY,
+         "virrz": oracle.F_VIRRZ, "nl": oracle.F_NHAT, "frho": oracle.F_FRHO}
 
 
 def golden_case(path):
@@ -38,7 +40,7 @@ def oracle_for(which, shape, params):
 
 
 def test_golden_files_present():
-    assert len(GOLDEN) >= 9
+    assert len(GOLDEN) >= 10
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
@@ -50,7 +52,7 @@ def test_oracle_matches_golden(path):
     o.set_psi(d["psi0"])
     l1 = []
     masses, energies = [], []
-    stepL1 = 50 if which == "quasi" else 100
+    stepL1 = 50 if which in ("quasi", "comp") else 100
     for s in range(1, steps + 1):
         o.step(1)
         if s % stepL1 == 0:
@@ -91,6 +93,7 @@ needs_ref = pytest.mark.skipif(not all(oracle.reference_available(w) for w in or
     ("quasi", (8, 12, 10), 6, dict(nw=8, dt=0.002, eps=-0.7, nu=1.0, kp=0.3, rho0=1.0, divv=2)),
     ("noadvc", (12, 10, 8), 30, dict(nw=8, dt=0.005, eps=-0.7)),
     ("advc", (10, 8, 12), 20, dict(nw=8, dt=0.005, eps=-0.7, nu=2.0)),
+    ("comp", (10, 12, 24), 12, dict(nw=8, dt=0.001, eps=-0.7, nu=1.5, rho0=0.05, zeta=0.002, rho_up=4, divv=5)),
 ])
 def test_oracle_matches_live_reference(which, shape, steps, params):
     rng = np.random.default_rng(99)
