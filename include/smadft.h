@@ -49,24 +49,32 @@ extern "C" {
 #define SMADFT_MODEL_NOADV 0  /* no-adv/cosNoAdvTrackSing.cpp */
 #define SMADFT_MODEL_ADV 1    /* adv/cosAdvTrackMult.cpp      */
 #define SMADFT_MODEL_QUASI 2  /* quasi/quasi.cpp              */
+#define SMADFT_MODEL_COMP 3   /* compressible/compressible.cpp (independent density, amplitude field) */
 
 #define SMADFT_FP64 0  /* every field and transform in double (the reference's arithmetic) */
 #define SMADFT_FP32 1  /* fields and transforms in float; FP64 reductions                 */
 
 #define SMADFT_FIELD_PSI 0       /* real-space psi                                              */
 #define SMADFT_FIELD_PSIHAT 1    /* scaled spectral psi, psi = REDFT01^3(psihat)                */
-#define SMADFT_FIELD_VX 2        /* real-space velocity of the last step (adv, quasi)           */
+#define SMADFT_FIELD_VX 2        /* real-space velocity of the last step (adv, quasi; comp: its
+                                    solenoidal part)                                             */
 #define SMADFT_FIELD_VY 3
 #define SMADFT_FIELD_VZ 4
 #define SMADFT_FIELD_GX 5        /* real-space grad psi of the last step (adv, quasi)           */
 #define SMADFT_FIELD_GY 6
 #define SMADFT_FIELD_GZ 7
-#define SMADFT_FIELD_RHO 8       /* quasi: filtered density of the last step                    */
+#define SMADFT_FIELD_RHO 8       /* quasi: filtered density of the last step; comp: the density  */
 #define SMADFT_FIELD_P 9         /* quasi: pressure of the last step                            */
-#define SMADFT_FIELD_DIVV 10     /* quasi: REDFT10^3 of div v (the reference keeps it spectral) */
+#define SMADFT_FIELD_DIVV 10     /* quasi: REDFT10^3 of div v (the reference keeps it spectral);
+                                    comp: div v in real space                                    */
 #define SMADFT_FIELD_MU 11       /* quasi: chemical potential of the last step                  */
-#define SMADFT_FIELD_ENERGY 12   /* quasi: energy density of the last step                      */
+#define SMADFT_FIELD_ENERGY 12   /* quasi: energy density of the last step (not comp)           */
 #define SMADFT_FIELD_NHAT 13     /* unscaled REDFT10^3 of the last nonlinear term               */
+#define SMADFT_FIELD_AMP 14      /* comp: Gaussian-filtered amplitude of the last step          */
+#define SMADFT_FIELD_VIRRX 15    /* comp: irrotational velocity of the last step                */
+#define SMADFT_FIELD_VIRRY 16
+#define SMADFT_FIELD_VIRRZ 17
+#define SMADFT_FIELD_FRHO 18     /* comp: density rate of the last step (its AB2 history)       */
 
 /* Interface tracker modes (reference trackers; the scan runs from the last index down) */
 #define SMADFT_TRACK_FLAT 0   /* psi > hi then psi < lo: no-adv/cosNoAdvTrackSing.cpp:880-913  */
@@ -76,7 +84,7 @@ extern "C" {
 
 /* Parameter block.  Mirrors the reference's compile-time constants and argv:
  * no-adv/cosNoAdvTrackSing.cpp:130-172, adv/cosAdvTrackMult.cpp:149-198,
- * quasi/quasi.cpp:203-268. */
+ * quasi/quasi.cpp:203-268, compressible/compressible.cpp:224-290. */
 typedef struct {
     int model;          /* SMADFT_MODEL_*                                             */
     int precision;      /* SMADFT_FP64 or SMADFT_FP32                                  */
@@ -93,7 +101,12 @@ typedef struct {
                          * no-adv/cosNoAdvConserv.cpp (L and N weighted by q^2) and
                          * adv/cosAdvConSingle.cpp (C1, C2 and the SH part of N weighted by
                          * q^2, the advection v.grad psi not); 0 = the non-conserved models */
-    int reserved[4];
+    int rho_up;         /* comp: planes rho is shifted up by in the relaxation steps (ref 16),
+                         * 0 <= rho_up < nz; comp uses rho0 as its rho_0 (ref 0.01), divv_switch
+                         * as the relaxation length, and derives Amp and kp from eps, beta, gamma */
+    int reserved[3];
+    double zeta;        /* comp: density penalty (ref 0.001)                                */
+    double reserved_d[3];
 } smadft_params;
 
 /* FP64 diagnostics of one step (no-adv/cosNoAdvTrackSing.cpp:769-801,

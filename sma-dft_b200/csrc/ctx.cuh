@@ -29,6 +29,7 @@ enum Slot : int {
     S_PSI = 0, S_PSI2, S_PSIH, S_PSIH_OLD, S_NP, S_TMP,
     S_GX, S_GY, S_GZ, S_SP2, S_SX, S_SY, S_SZ, S_VX, S_VY, S_VZ,
     S_RHO, S_RHO_OLD, S_RHOQ, S_DFD, S_RDX, S_RDY, S_RDZ, S_LAP, S_DIVV, S_P, S_MU, S_EN,
+    S_AMP, S_FRHO, S_FGRAD, S_FX, S_FY, S_FZ, S_VIRX, S_VIRY, S_VIRZ, S_AMPD,   // compressible
     S_COUNT
 };
 
@@ -51,6 +52,7 @@ struct Spec {
     const T *ex, *ey, *ez;                   // exp(-2 * 1.57^2 q^2) per axis (quasi filter)
     T eps, alpha, beta, gamma, q02, dtd2, dt, scale, nu;
     T rho_m, lam, kp, rho0;
+    T zeta, amp0;                            // compressible: density penalty, one-mode amplitude
     int nx, ny, nz;
     int nyz;
     __device__ __forceinline__ T mq2(int i, int j, int k) const
@@ -137,6 +139,15 @@ Spec<T> make_spec(const Ctx &c)
     s.nu = T(p.nu);
     double rho_s = p.kp * p.amp + p.rho0;       // quasi/quasi.cpp:244-245
     s.rho_m = T(rho_s / 2); s.lam = T(-2 * p.nu / 3); s.kp = T(p.kp); s.rho0 = T(p.rho0);
+    s.zeta = T(p.zeta); s.amp0 = T(p.amp);
+    if (p.model == SMADFT_MODEL_COMP) {
+        // compressible/compressible.cpp:265-271: Amp of the one-mode smectic at eps, kp so that
+        // rho_s = kp Amp + rho_0 = 1, rho_m = rho_s / 2, lambda = nu
+        const double amp = std::sqrt((3 * p.beta + std::sqrt(9 * p.beta * p.beta + 40 * p.eps * p.gamma)) / 5);
+        const double kp = (1 - p.rho0) / amp;
+        rho_s = kp * amp + p.rho0;
+        s.rho_m = T(rho_s / 2); s.lam = T(p.nu); s.kp = T(kp); s.amp0 = T(amp);
+    }
     s.nx = c.g.nx; s.ny = c.g.ny; s.nz = c.g.nz; s.nyz = c.g.nyz;
     return s;
 }

@@ -132,14 +132,21 @@ std::vector<int> slots_for(int model)
                       S_DIVV, S_P, S_MU, S_EN})
             s.push_back(q);
     }
+    if (model == SMADFT_MODEL_COMP) {
+        for (int q : {S_PSIH_OLD, S_RHO, S_RHOQ, S_DFD, S_RDX, S_RDY, S_RDZ, S_LAP, S_DIVV, S_MU, S_EN,
+                      S_AMP, S_FRHO, S_FGRAD, S_FX, S_FY, S_FZ, S_VIRX, S_VIRY, S_VIRZ, S_AMPD})
+            s.push_back(q);
+    }
     return s;
 }
 
 // Graph variant of the next loop body (see StepGraph).
 int step_variant(const Ctx &c)
 {
-    if (c.p.model != SMADFT_MODEL_QUASI) return 0;
+    if (c.p.model != SMADFT_MODEL_QUASI && c.p.model != SMADFT_MODEL_COMP) return 0;
     const long long nloop = c.steps + 1;
+    if (c.p.model == SMADFT_MODEL_COMP)
+        return (nloop == 1) | ((nloop > c.p.divv_switch || c.p.loaded) ? 2 : 0);
     const int first = nloop == 1;
     const int divv = (nloop > c.p.divv_switch || c.p.loaded) ? 1 : 0;
     const int extra = nloop > c.p.divv_switch + 1;
@@ -153,6 +160,7 @@ int one_step(Ctx &c, bool keep_old)
     switch (c.p.model) {
     case SMADFT_MODEL_NOADV: rc = noadv_step<T>(c, keep_old); break;
     case SMADFT_MODEL_ADV: rc = adv_step<T>(c); break;
+    case SMADFT_MODEL_COMP: rc = comp_step<T>(c, c.steps + 1, keep_old); break;
     default: rc = quasi_step<T>(c, c.steps + 1, keep_old); break;
     }
     return rc;
@@ -202,6 +210,8 @@ int finish_diag(Ctx &c, smadft_diag *out)
     double ms[2] = {0, 0};
     if (c.p.model == SMADFT_MODEL_QUASI) {
         if ((rc = reduce_mass_energy<T>(c, ms))) return rc;
+    } else if (c.p.model == SMADFT_MODEL_COMP) {
+        if ((rc = reduce_comp_mass_energy<T>(c, nw, ms))) return rc;
     }
     // psi_new -> S_PSI by copy: captured step graphs hold the slot pointers
     SMADFT_CUDA(cudaMemcpyAsync(c.slot[S_PSI], c.slot[S_PSI2], c.esize * c.n, cudaMemcpyDeviceToDevice, c.stream));
@@ -334,7 +344,13 @@ void smadft_params_init(smadft_params *p, int model)
     p->alpha = 1.0; p->beta = 2.0; p->gamma = 1.0; p->eps = -0.75; p->q0 = 1.0;
     p->nu = 1.0;
     p->rho0 = 1.0; p->kp = 0.0; p->amp = 1.34164;   // quasi/quasi.cpp:241-243
-    p->divv_switch = 200;                            // quasi/quasi.cpp:206
+    p->divv_switch = 200;                            // quasi/quasi.cpp:206, compressible/compressible.cpp:228
+    if (model == SMADFT_MODEL_COMP) {                // compressible/compressible.cpp:229,266,272,279
+        p->dt = 0.001;
+        p->rho0 = 0.01;
+        p->zeta = 0.001;
+        p->rho_up = 16;
+    }
     p->loaded = 0;
     p->device = 0;
 }
@@ -342,7 +358,7 @@ void smadft_params_init(smadft_params *p, int model)
 int smadft_params_check(const smadft_params *p)
 {
     if (!p) return SMADFT_ERR_INVALID;
-    if (p->model < 0 || p->model > 2) return SMADFT_ERR_INVALID;
+    if (p->model < 0 || p->model > 3) return SMADFT_ERR_INVALID;
     if (p->precision != SMADFT_FP64 && p->precision != SMADFT_FP32) return SMADFT_ERR_INVALID;
     if (p->nx < 4 || p->ny < 4 || p->nz < 4) return SMADFT_ERR_INVALID;
     if (p->nx > 1024 || p->ny > 1024 || p->nz > 1024) return SMADFT_ERR_UNSUPPORTED;
@@ -351,7 +367,14 @@ int smadft_params_check(const smadft_params *p)
     if (p->model != SMADFT_MODEL_NOADV && !(p->nu > 0)) return SMADFT_ERR_INVALID;
     if (p->model == SMADFT_MODEL_QUASI && !(p->rho0 > 0)) return SMADFT_ERR_INVALID;
     // the reference has conserved variants of noadv and adv only
-    if (p->conserved != 0 && (p->conserved != 1 || p->model == SMADFT_MODEL_QUASI)) return SMADFT_ERR_INVALID;
+    if (p->conserved != 0 && (p->conserved != 1 || p->model >= SMADFT_MODEL_QUASI)) return SMADFT_ERR_INVALID;
+    if (p->model == SMADFT_MODEL_COMP) {
+        if (!(p->rho0 >= 0 && p->rho0 < 1) || !(p->zeta >= 0) || p->rho_up < 0 || p->rho_up >= p->nz)
+            return SMADFT_ERR_INVALID;
+        // the reference's load == 1 branch also reads rho from files; this ABI has no rho input
+        if (p->loaded) return SMADFT_ERR_UNSUPPORTED;
+        if (!(9 * p->beta * p->beta + 40 * p->eps * p->gamma >= 0)) return SMADFT_ERR_INVALID;   // real Amp
+    }
     return SMADFT_OK;
 }
 
@@ -499,6 +522,11 @@ int smadft_get_field(smadft_ctx *h, int field, double *host, size_t n)
     case SMADFT_FIELD_MU: slot = S_MU; break;
     case SMADFT_FIELD_ENERGY: slot = S_EN; break;
     case SMADFT_FIELD_NHAT: slot = S_NP; break;
+    case SMADFT_FIELD_AMP: slot = S_AMP; break;
+    case SMADFT_FIELD_VIRRX: slot = S_VIRX; break;
+    case SMADFT_FIELD_VIRRY: slot = S_VIRY; break;
+    case SMADFT_FIELD_VIRRZ: slot = S_VIRZ; break;
+    case SMADFT_FIELD_FRHO: slot = S_FRHO; break;
     default: return fail(c, SMADFT_ERR_INVALID, "unknown field");
     }
     if (!c.slot[slot]) return fail(c, SMADFT_ERR_INVALID, "field not available for this model");
@@ -572,7 +600,7 @@ int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH
     if (!h || !surf_idx || !vel || !curvH || !curvK) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
-    if (c.p.model == SMADFT_MODEL_QUASI) return fail(c, SMADFT_ERR_UNSUPPORTED, "surface diagnostics: noadv and adv");
+    if (c.p.model >= SMADFT_MODEL_QUASI) return fail(c, SMADFT_ERR_UNSUPPORTED, "surface diagnostics: noadv and adv");
     if (c.p.conserved) return fail(c, SMADFT_ERR_UNSUPPORTED, "surface diagnostics: non-conserved runs only");
     cudaSetDevice(c.dev);
     SurfaceScratch &sc = h->surf;
@@ -609,7 +637,7 @@ int smadft_adjoint(smadft_ctx *h, const smadft_adj_opts *o, smadft_grads *out, d
         return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if (!c.have_psi || c.steps != 0) return fail(c, SMADFT_ERR_STATE, "adjoint: start from the initial condition");
-    if (c.p.model == SMADFT_MODEL_QUASI || c.p.conserved)
+    if (c.p.model >= SMADFT_MODEL_QUASI || c.p.conserved)
         return fail(c, SMADFT_ERR_UNSUPPORTED, "adjoint: non-conserved noadv and adv only");
     cudaSetDevice(c.dev);
     std::memset(out, 0, sizeof(*out));

@@ -39,6 +39,7 @@ int pre_loop(Ctx &c)
     T *np = c.f<T>(S_NP);
     int rc;
     if (c.p.model == SMADFT_MODEL_QUASI) return quasi_pre_loop<T>(c);
+    if (c.p.model == SMADFT_MODEL_COMP) return comp_pre_loop<T>(c);
     // psihat = scale REDFT10^3 psi ; Nprev = REDFT10^3(beta psi^3 - gamma psi^5) (no advection)
     // no-adv/cosNoAdvTrackSing.cpp:618-635, adv/cosAdvTrackMult.cpp:760-777; weighted by q^2
     // for conserved noadv (no-adv/cosNoAdvConserv.cpp:688-701), unweighted for conserved adv

@@ -14,6 +14,11 @@ template <typename T> int adv_step(Ctx &c);
 template <typename T> int adv_fields(Ctx &c);
 // quasi/quasi.cpp:1099-2190 (nloop = 1-based step counter)
 template <typename T> int quasi_step(Ctx &c, long long nloop, bool keep_old);
+// compressible/compressible.cpp:1265-2720 (nloop = 1-based step counter); its pre-loop block
+// (:1104-1135) and the mass / energy sums of a step (:2642-2690, psi_new = the step's psi)
+template <typename T> int comp_step(Ctx &c, long long nloop, bool keep_old);
+template <typename T> int comp_pre_loop(Ctx &c);
+template <typename T> int reduce_comp_mass_energy(Ctx &c, const T *psi_new, double *ms);
 // pre-loop blocks: no-adv :618-635, adv :760-777, quasi :990-1062
 template <typename T> int pre_loop(Ctx &c);
 // psi = REDFT01^3 psihat into dst

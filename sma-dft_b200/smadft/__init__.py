@@ -16,10 +16,10 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "libsmadft.so")
 
-NOADV, ADV, QUASI = 0, 1, 2
+NOADV, ADV, QUASI, COMP = 0, 1, 2, 3
 FP64, FP32 = 0, 1
 FIELD = dict(psi=0, psihat=1, vx=2, vy=3, vz=4, gx=5, gy=6, gz=7, rho=8, p=9, divv=10, mu=11,
-             energy=12, nhat=13)
+             energy=12, nhat=13, amp=14, virrx=15, virry=16, virrz=17, frho=18)
 TRACK_FLAT, TRACK_BUMP, TRACK_LEVEL = 0, 1, 2
 REDFT10, REDFT01, RODFT10, RODFT01 = 0, 1, 2, 3
 
@@ -46,7 +46,8 @@ class Params(ctypes.Structure):
         ("eps", ctypes.c_double), ("q0", ctypes.c_double), ("nu", ctypes.c_double),
         ("rho0", ctypes.c_double), ("kp", ctypes.c_double), ("amp", ctypes.c_double),
         ("divv_switch", ctypes.c_int), ("loaded", ctypes.c_int), ("device", ctypes.c_int),
-        ("conserved", ctypes.c_int), ("reserved", ctypes.c_int * 4),
+        ("conserved", ctypes.c_int), ("rho_up", ctypes.c_int), ("reserved", ctypes.c_int * 3),
+        ("zeta", ctypes.c_double), ("reserved_d", ctypes.c_double * 3),
     ]
 
 

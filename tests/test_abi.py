@@ -73,7 +73,18 @@ def test_conserved_flag_only_for_noadv_and_adv(smadft_lib):
         assert smadft_lib.smadft_params_check(ctypes.byref(p)) == -1
     p = smadft.params(smadft.QUASI, (16, 16, 16), conserved=1)
     assert smadft_lib.smadft_params_check(ctypes.byref(p)) == -1
-    assert ctypes.sizeof(smadft.Params) == 144       # the flag took a reserved slot
+    assert ctypes.sizeof(smadft.Params) == 176       # conserved and rho_up in reserved ints, then zeta
+
+
+def test_comp_parameter_checks(smadft_lib):
+    p = smadft.params(smadft.COMP, (16, 16, 24))
+    assert (p.dt, p.rho0, p.zeta, p.rho_up) == (0.001, 0.01, 0.001, 16)
+    assert smadft_lib.smadft_params_check(ctypes.byref(p)) == 0
+    p.rho_up = 24                        # must stay below nz
+    assert smadft_lib.smadft_params_check(ctypes.byref(p)) == -1
+    p.rho_up = 16
+    p.loaded = 1                         # the reference's load branch also reads rho from files
+    assert smadft_lib.smadft_params_check(ctypes.byref(p)) == -6
 
 
 def test_error_strings(smadft_lib):

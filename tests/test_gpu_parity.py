@@ -16,11 +16,13 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
 MODEL = {"noadv": smadft.NOADV, "bump": smadft.NOADV, "adv": smadft.ADV, "quasi": smadft.QUASI,
-         "noadvc": smadft.NOADV, "advc": smadft.ADV}
+         "noadvc": smadft.NOADV, "advc": smadft.ADV, "comp": smadft.COMP}
 CONSERVED = {"noadvc", "advc"}
 OMODEL = {smadft.NOADV: oracle.NOADV, smadft.ADV: oracle.ADV, smadft.QUASI: oracle.QUASI}
 GFIELD = {"psi": "psi", "nq": "nhat", "vx": "vx", "vy": "vy", "vz": "vz", "gx": "gx", "gy": "gy",
-          "gz": "gz", "rho": "rho", "p": "p", "mu": "mu", "energy": "energy", "psiq": "psihat"}
+          "gz": "gz", "rho": "rho", "p": "p", "mu": "mu", "energy": "energy", "psiq": "psihat",
+          "amp": "amp", "divv": "divv", "vsolx": "vx", "vsoly": "vy", "vsolz": "vz", "virrx": "virrx",
+          "virry": "virry", "virrz": "virrz", "nl": "nhat", "frho": "frho"}
 
 
 def rel_max(a, b):
@@ -34,6 +36,8 @@ def rel_l2(a, b):
 def solver_for(which, shape, params, precision=smadft.FP64):
     kw = dict(params)
     divv = int(kw.pop("divv", 200))
+    if "rho_up" in kw:
+        kw["rho_up"] = int(kw["rho_up"])
     p = smadft.params(MODEL[which], shape, precision=precision, divv_switch=divv,
                       conserved=int(which in CONSERVED), **kw)
     return smadft.Solver(p)
@@ -48,7 +52,7 @@ def test_fp64_matches_golden(path):
     params = dict(zip([str(k) for k in d["params_keys"]], [float(v) for v in d["params_vals"]]))
     shape = tuple(int(s) for s in d["shape"])
     steps = int(d["steps"])
-    stepL1 = 50 if which == "quasi" else 100
+    stepL1 = 50 if which in ("quasi", "comp") else 100
     with solver_for(which, shape, params) as s:
         s.set_psi(d["psi0"])
         l1, mass, energy = [], [], []
