@@ -149,7 +149,7 @@ orc_ctx *orc_create(const orc_params *p)
                     c->C2[idx] = (1.0 - dtd2 * c->aLin[idx]);
                 }
                 if (p->model == ORC_COMP) {
-                    /* compressible/compressible.cpp:1092-1100: CM1 = scale/|q_s|^2 (nu applied later) */
+                    /* compressible/compressible.cpp:1136-1145: CM1 = scale/|q_s|^2 (nu applied later) */
                     double m2 = pow(c->sx[i], 2) + pow(c->qy[j], 2) + pow(c->qz[k], 2);
                     c->CM1x[idx] = c->scale / (m2);
                     c->CM2x[idx] = c->sx[i] / m2;
@@ -205,9 +205,9 @@ int orc_set_psi(orc_ctx *c, const double *psi0)
     c->nloop = 0;
     c->L1 = c->mass = c->en = 0.0;
     if (c->p.model == ORC_COMP) {
-        /* compressible/compressible.cpp:1104-1135: psiq = s CT(psi), psi = iCT(psiq), N^0
+        /* compressible/compressible.cpp:1150-1194: psiq = s CT(psi), psi = iCT(psiq), N^0
          * (unused: the first step sets Nl_old = Nl), psiq_old, psi_old; rho and its rate start
-         * at zero (load != 1, :579-580) */
+         * at zero (load != 1, :612) */
         r3(c, c->psi, c->psiq, T10, T10, T10);
         for (long q = 0; q < n; q++) c->psiq[q] = c->scale * c->psiq[q];
         r3(c, c->psiq, c->psi, T01, T01, T01);
@@ -621,11 +621,11 @@ static void step_comp(orc_ctx *c)
     const double beta = P->beta, gamma = P->gamma, alpha = P->alpha, ep = P->eps;
     const double q02 = P->q0 * P->q0, nu = P->nu, lambda = c->lambda, zeta = P->zeta;
     const double rho_0 = P->rho0, kp = c->kp_c, Amp = c->amp_c;
-    c->nloop++;                                                      /* :1268 */
+    c->nloop++;                                                      /* :1269 */
     const long nLoop = c->nloop;
-    memcpy(c->NqPast, c->Nq, sizeof(double) * n);                    /* :1283 Nl_old = Nl */
-    r3(c, c->rho, c->rhoq, T10, T10, T10);                           /* :1287-1289 */
-    /* shifted gradient spectra of psi and rho (:1290-1388) */
+    memcpy(c->NqPast, c->Nq, sizeof(double) * n);                    /* :1287 Nl_old = Nl */
+    r3(c, c->rho, c->rhoq, T10, T10, T10);                           /* :1292-1294 */
+    /* shifted gradient spectra of psi and rho (:1296-1431) */
     memset(c->gx, 0, sizeof(double) * n); memset(c->gy, 0, sizeof(double) * n); memset(c->gz, 0, sizeof(double) * n);
     memset(c->rdx, 0, sizeof(double) * n); memset(c->rdy, 0, sizeof(double) * n); memset(c->rdz, 0, sizeof(double) * n);
     for (int i = 0; i < nx; i++)
@@ -645,22 +645,22 @@ static void step_comp(orc_ctx *c)
                     c->rdz[q] = -scale * c->sz[k] * c->rhoq[q + 1];
                 }
             }
-    r3(c, c->gx, c->gx, S01, T01, T01);                              /* :1390-1408 */
+    r3(c, c->gx, c->gx, S01, T01, T01);                              /* :1433-1455 */
     r3(c, c->gy, c->gy, T01, S01, T01);
     r3(c, c->gz, c->gz, T01, T01, S01);
     r3(c, c->rdx, c->rdx, S01, T01, T01);
     r3(c, c->rdy, c->rdy, T01, S01, T01);
     r3(c, c->rdz, c->rdz, T01, T01, S01);
-    /* amplitude, Gaussian-filtered (:1420-1456) */
+    /* amplitude, Gaussian-filtered (:1478-1515) */
     for (long q = 0; q < n; q++)
         c->amp[q] = sqrt(q02 * pow(c->psi[q], 2) + pow(c->gx[q], 2) + pow(c->gy[q], 2) + pow(c->gz[q], 2));
     r3(c, c->amp, c->amp, T10, T10, T10);
     for (long q = 0; q < n; q++) c->amp[q] = scale * c->amp[q] * exp(-1.57 * 1.57 * c->mq2[q] * 2);
     r3(c, c->amp, c->amp, T01, T01, T01);
-    /* dF/d(lap psi) (:1460-1474) */
+    /* dF/d(lap psi) (:1520-1534) */
     for (long q = 0; q < n; q++) c->dfd[q] = alpha * (q02 - c->mq2[q]) * c->psiq[q];
     r3(c, c->dfd, c->dfd, T01, T01, T01);
-    /* lap(rho dF/dlap psi) (:1478-1560): after the relaxation steps rho is independent;
+    /* lap(rho dF/dlap psi) (:1542-1630): after the relaxation steps rho is independent;
      * during them rho follows the amplitude, shifted up by rho_up planes */
     if (nLoop > P->divv_switch || P->loaded) {
         for (long q = 0; q < n; q++) c->lap[q] = c->rho[q] * c->dfd[q];
@@ -691,7 +691,7 @@ static void step_comp(orc_ctx *c)
                 }
         }
     }
-    /* forces, chemical potential, density penalty (:1564-1610) */
+    /* forces, chemical potential, density penalty (:1636-1678) */
     for (long q = 0; q < n; q++) {
         c->energy[q] = 0.5 * pow(c->dfd[q], 2);
         c->fgrad[q] = 0.5 * zeta * (pow(c->rho[q], 2) - pow(rho_0 + kp * c->amp[q], 2));
@@ -707,7 +707,7 @@ static void step_comp(orc_ctx *c)
         c->fys[q] = fx * c->gy[q];
         c->fzs[q] = fx * c->gz[q];
     }
-    r3(c, c->fgrad, c->fgrad, T10, T10, T10);                        /* :1614-1700 */
+    r3(c, c->fgrad, c->fgrad, T10, T10, T10);                        /* :1681-1711 */
     r3(c, c->energy, c->energy, T10, T10, T10);
     r3(c, c->Sx, c->Sx, S10, T10, T10);
     r3(c, c->Sy, c->Sy, T10, S10, T10);
@@ -769,29 +769,29 @@ static void step_comp(orc_ctx *c)
     r3(c, c->virx, c->virx, S01, T01, T01);
     r3(c, c->viry, c->viry, T01, S01, T01);
     r3(c, c->virz, c->virz, T01, T01, S01);
-    /* mass balance, AB2 in real space (:2556-2572) */
+    /* mass balance, AB2 in real space (:2555-2573) */
     for (long q = 0; q < n; q++) {
         const double S = -(c->vx[q] + c->virx[q]) * c->rdx[q] - (c->vy[q] + c->viry[q]) * c->rdy[q] -
                          (c->vz[q] + c->virz[q]) * c->rdz[q] - c->rho[q] * c->divv[q];
         c->rho[q] = c->rho[q] + dt * (1.5 * S - 0.5 * c->frho[q]);
         c->frho[q] = S;
     }
-    /* N (:2576-2596) */
+    /* N (:2578-2612) */
     for (long q = 0; q < n; q++)
         c->Nr[q] = -c->mu[q] + (kp * zeta / (c->amp[q] + 0.001)) * (c->rho[q] - rho_0 - kp * c->amp[q]) * c->psi[q] -
                    c->ampd[q] - (c->vx[q] + c->virx[q]) * c->gx[q] - (c->vy[q] + c->viry[q]) * c->gy[q] -
                    (c->vz[q] + c->virz[q]) * c->gz[q];
-    r3(c, c->Nr, c->Nq, T10, T10, T10);                              /* :2600-2602 */
-    if (nLoop == 1) memcpy(c->NqPast, c->Nq, sizeof(double) * n);    /* :2604-2606 */
-    for (long q = 0; q < n; q++) {                                   /* :2618-2629 */
+    r3(c, c->Nr, c->Nq, T10, T10, T10);                              /* :2613 */
+    if (nLoop == 1) memcpy(c->NqPast, c->Nq, sizeof(double) * n);    /* :2615-2617 */
+    for (long q = 0; q < n; q++) {                                   /* :2619-2635 */
         const double old = c->psiq[q];
         c->psiq[q] = (c->C1[q] * c->psiq[q] - 0.5 * c->psiq_old[q] +
                       dtd2 * scale * (3.0 * c->Nq[q] - c->NqPast[q])) / c->C2[q];
         c->psiq_old[q] = old;
     }
-    memcpy(c->psi_old, c->psi, sizeof(double) * n);                  /* :2633 */
-    r3(c, c->psiq, c->psi, T01, T01, T01);                           /* :2635-2637 */
-    /* diagnostics (:2642-2690), every step here */
+    memcpy(c->psi_old, c->psi, sizeof(double) * n);                  /* :2639 */
+    r3(c, c->psiq, c->psi, T01, T01, T01);                           /* :2641-2643 */
+    /* diagnostics (:2647-2690), every step here */
     c->L1 = l1_measure(c, c->psi, c->psi_old);
     double rs = 0.0, es = 0.0;
     for (long q = 0; q < n; q++) {

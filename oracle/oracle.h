@@ -8,7 +8,7 @@
  *   ORC_NOADV  no-adv/cosNoAdvTrackSing.cpp:584-1074   (diffusive, CN/AB2)
  *   ORC_ADV    adv/cosAdvTrackMult.cpp:717-1744          (advected, Stokes projection)
  *   ORC_QUASI  quasi/quasi.cpp:951-2498                  (quasi-incompressible, BDF2-like)
- *   ORC_COMP   compressible/compressible.cpp:1079-2720   (independent density, amplitude field)
+ *   ORC_COMP   compressible/compressible.cpp:1122-2720   (independent density, amplitude field)
  *
  * Parity is pinned two ways (tests/test_oracle_pin.py): against the reference's own
  * sources compiled here with a single-rank MPI shim and an FFTW-r2r shim (oracle/_ref,

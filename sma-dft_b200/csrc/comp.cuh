@@ -12,7 +12,7 @@
 namespace smadft {
 
 // T(scale) times a forward transform: rhohat for the gradient spectra of rho
-// (compressible/compressible.cpp:1287-1388 scale the shifted rhohat by `scale`)
+// (compressible/compressible.cpp:1292-1431 scale the shifted rhohat by `scale`)
 template <typename T>
 struct StScaleT {
     T *__restrict__ out;
@@ -35,7 +35,7 @@ struct StScaleT {
     }
 };
 
-// Relaxation steps (:1512-1557): rho = rho_0 + ((1 - rho_0)/Amp) A, lap *= rho; then rho is
+// Relaxation steps (:1574-1630): rho = rho_0 + ((1 - rho_0)/Amp) A, lap *= rho; then rho is
 // shifted up by `up` planes in z (rho = 1 below) and lap multiplied by the shifted rho once
 // more, as the reference's second loop does.  Out of place in rho, in place in lap.
 template <typename T>
@@ -55,7 +55,7 @@ __global__ void comp_relax_kernel(int nz, int up, long long n, T rho1, T c1, con
     }
 }
 
-// The eight forward-transformed fields of :1564-1700, all from psi, f' (dfd), lap, rho, A:
+// The eight forward-transformed fields of :1636-1711, all from psi, f' (dfd), lap, rho, A:
 //   C 0  fgrad = zeta/2 (rho^2 - (rho_0 + kp A)^2)        (also stores mu)
 //   C 1  e = rho f'^2 / 2
 //   C 2-4  S_c = (lap + rho f') d_c psi + f'^2/2 d_c rho   (c = C - 2)
@@ -172,7 +172,7 @@ __global__ void comp_div_kernel(Spec<T> s, const T *__restrict__ vix, const T *_
     }
 }
 
-// Mass balance, AB2 in real space (:2556-2572):
+// Mass balance, AB2 in real space (:2555-2573):
 //   S = -(vsol + virr) . grad rho - rho div v,  rho += dt (3/2 S - 1/2 S_prev),  S_prev = S
 template <typename T>
 __global__ void comp_rho_kernel(long long n, T dt, const T *__restrict__ vsx, const T *__restrict__ vsy,
@@ -190,7 +190,7 @@ __global__ void comp_rho_kernel(long long n, T dt, const T *__restrict__ vsx, co
 }
 
 // N = -mu + kp zeta/(A + 0.001) (rho - rho_0 - kp A) psi - ampd - (vsol + virr) . grad psi
-// (:2576-2596)
+// (:2578-2612)
 template <typename T>
 struct LdCN {
     static constexpr int kMinBlocks = 2;
@@ -221,7 +221,7 @@ struct LdCN {
 };
 
 // sums of rho and of rho e + zeta/2 (rho - rho_0 - kp A)^2 with the energy density
-// e = -eps psi^2/2 + f'^2/2 - beta psi^4/4 + gamma psi^6/6 of the new psi (:2642-2690)
+// e = -eps psi^2/2 + f'^2/2 - beta psi^4/4 + gamma psi^6/6 of the new psi (:2647-2690)
 template <typename T>
 struct RedCompME {
     const T *__restrict__ psi, *__restrict__ dfd, *__restrict__ rho, *__restrict__ amp;
@@ -239,8 +239,8 @@ struct RedCompME {
 template <typename T>
 int comp_pre_loop(Ctx &c)
 {
-    // psihat = scale CT(psi), psi = iCT(psihat), psihat_old = psihat (:1104-1135); rho and its
-    // AB2 history start at zero (:579-580)
+    // psihat = scale CT(psi), psi = iCT(psihat), psihat_old = psihat (:1150-1194); rho and its
+    // AB2 history start at zero (:612)
     int rc = quasi_pre_loop<T>(c);
     if (rc) return rc;
     SMADFT_CUDA(cudaMemsetAsync(c.slot[S_RHO], 0, c.esize * c.n, c.stream));
@@ -267,7 +267,7 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
     T *vsx = c.f<T>(S_VX), *vsy = c.f<T>(S_VY), *vsz = c.f<T>(S_VZ);
     T *vix = c.f<T>(S_VIRX), *viy = c.f<T>(S_VIRY), *viz = c.f<T>(S_VIRZ);
     int rc;
-    // scale CT(rho) (:1287-1289), then f', grad psi (from psihat) and grad rho (:1290-1474)
+    // scale CT(rho) (:1292-1294), then f', grad psi (from psihat) and grad rho (:1296-1534)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LoadArr<T>{rho}, StScaleT<T>{rq, s.scale}))) return rc;
     {
         const int kx[4] = {K_DCT3, K_DST3, K_DCT3, K_DCT3};
@@ -286,11 +286,11 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
         if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdGrad<T, 0>{s, rq}, LdGrad<T, 1>{s, rq}, LdGrad<T, 2>{s, rq})))
             return rc;
     }
-    // amplitude: filtered sqrt(q0^2 psi^2 + |grad psi|^2) (:1420-1456), via rq (free now)
+    // amplitude: filtered sqrt(q0^2 psi^2 + |grad psi|^2) (:1478-1515), via rq (free now)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdRhoRaw<T>{psi, gx, gy, gz, T(1), T(0), s.q02},
                        StFilter<T>{s, rq}))) return rc;
     if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{rq}, StoreArr<T>{amp}))) return rc;
-    // lap(rho f') (:1478-1560)
+    // lap(rho f') (:1542-1630)
     if (nloop > P.divv_switch || P.loaded) {
         if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2, LdMul<T>{rho, dfd}, StLapSpec<T>{s, lap}))) return rc;
         if ((rc = r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T>{lap}, StoreArr<T>{lap}))) return rc;
@@ -302,7 +302,7 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
         SMADFT_CUDA(cudaGetLastError());
         c.launches++;
     }
-    // fgrad, e, S and the penalty force f, forward (:1564-1700); the first loader stores mu
+    // fgrad, e, S and the penalty force f, forward (:1636-1711); the first loader stores mu
     {
         const int kx[8] = {K_DCT2, K_DCT2, K_DST2, K_DCT2, K_DCT2, K_DST2, K_DCT2, K_DCT2};
         const int ky[8] = {K_DCT2, K_DCT2, K_DCT2, K_DST2, K_DCT2, K_DCT2, K_DST2, K_DCT2};
@@ -342,16 +342,16 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
                                            LoadArr<T>{ad})))
             return rc;
     }
-    // mass balance (:2556-2572)
+    // mass balance (:2555-2573)
     comp_rho_kernel<T><<<c.red_blocks, 256, 0, c.stream>>>(n, s.dt, vsx, vsy, vsz, vix, viy, viz, rx, ry, rz, dv,
                                                            rho, fr);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
-    // N and the BDF2-like update (:2576-2629)
+    // N and the BDF2-like update (:2578-2635)
     if ((rc = r2r3d<T>(c, K_DCT2, K_DCT2, K_DCT2,
                        LdCN<T>{mu, amp, rho, psi, ad, vsx, vsy, vsz, vix, viy, viz, gx, gy, gz, s.kp, s.zeta, s.rho0},
                        StUpdBDF<T>{make_spec<double>(c), ph, pho, np, (int)(nloop == 1)}))) return rc;
-    // psi = iCT(psihat) (:2633-2637)
+    // psi = iCT(psihat) (:2639-2643)
     T *dst = keep_old ? c.f<T>(S_PSI2) : psi;
     return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T, double>{ph}, StoreArr<T>{dst});
 }

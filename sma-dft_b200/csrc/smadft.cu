@@ -345,7 +345,7 @@ void smadft_params_init(smadft_params *p, int model)
     p->nu = 1.0;
     p->rho0 = 1.0; p->kp = 0.0; p->amp = 1.34164;   // quasi/quasi.cpp:241-243
     p->divv_switch = 200;                            // quasi/quasi.cpp:206, compressible/compressible.cpp:228
-    if (model == SMADFT_MODEL_COMP) {                // compressible/compressible.cpp:229,266,272,279
+    if (model == SMADFT_MODEL_COMP) {                // compressible/compressible.cpp:229,266,272,277
         p->dt = 0.001;
         p->rho0 = 0.01;
         p->zeta = 0.001;

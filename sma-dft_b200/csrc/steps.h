@@ -15,7 +15,7 @@ template <typename T> int adv_fields(Ctx &c);
 // quasi/quasi.cpp:1099-2190 (nloop = 1-based step counter)
 template <typename T> int quasi_step(Ctx &c, long long nloop, bool keep_old);
 // compressible/compressible.cpp:1265-2720 (nloop = 1-based step counter); its pre-loop block
-// (:1104-1135) and the mass / energy sums of a step (:2642-2690, psi_new = the step's psi)
+// (:1150-1194) and the mass / energy sums of a step (:2647-2690, psi_new = the step's psi)
 template <typename T> int comp_step(Ctx &c, long long nloop, bool keep_old);
 template <typename T> int comp_pre_loop(Ctx &c);
 template <typename T> int reduce_comp_mass_energy(Ctx &c, const T *psi_new, double *ms);

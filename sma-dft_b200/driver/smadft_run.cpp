@@ -7,10 +7,14 @@
 // energy.dat (quasi/quasi.cpp:2232-2248), info (quasi/quasi.cpp:820-843), and the per-rank
 // text save psi0.dat (adv/cosAdvTrackMult.cpp:1546-1557) which `ic=file:` reads back.
 //
-// usage: smadft_run noadv|adv|quasi [nu e0d radius load] [key=value ...]
+// comp (compressible/compressible.cpp) also writes rhoMid.dat and amp.dat mid slices
+// (:2885-2892) and rho0.dat at the end (:2786-2799), and tracks rho > rho_s - 0.15 (:2734).
+//
+// usage: smadft_run noadv|adv|quasi|comp [nu e0d radius load] [key=value ...]
 //   keys: n nx ny nz nw dt eps alpha beta gamma nu kp rho0 divv steps l1every saveevery
 //         precision(fp64|fp32) conserved(0|1) ic(interface|bump|focal|conics|file:<path>) A
 //         radius seed noise out track_axis track_mode track_hi track_lo checkpoint resume
+//         zeta rhoup (comp)
 // conserved=1 runs the reference's conserved variants (no-adv/cosNoAdvConserv.cpp,
 // adv/cosAdvConSingle.cpp); their save iteration writes surfPsi.dat but no velSurf/curvH/curvK
 // values (the library has no conserved surface diagnostics).
@@ -63,12 +67,12 @@ void append_slice(const std::string &path, const std::vector<double> &f, int nx,
 int main(int argc, char **argv)
 {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: %s noadv|adv|quasi [nu e0d radius load] [key=value ...]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s noadv|adv|quasi|comp [nu e0d radius load] [key=value ...]\n", argv[0]);
         return 2;
     }
     std::string model = argv[1];
     int m = model == "noadv" ? SMADFT_MODEL_NOADV : model == "adv" ? SMADFT_MODEL_ADV
-          : model == "quasi" ? SMADFT_MODEL_QUASI : -1;
+          : model == "quasi" ? SMADFT_MODEL_QUASI : model == "comp" ? SMADFT_MODEL_COMP : -1;
     if (m < 0) { std::fprintf(stderr, "unknown model %s\n", argv[1]); return 2; }
     Opt o;
     std::vector<std::string> pos;
@@ -83,7 +87,7 @@ int main(int argc, char **argv)
     // reference argv: nu, eps = -0.01 arg (adv) or -0.001 arg (quasi), radius, load
     // (adv/cosAdvTrackMult.cpp:127,160-177; quasi/quasi.cpp:173,221-240)
     if (pos.size() >= 1) p.nu = std::atof(pos[0].c_str());
-    if (pos.size() >= 2) p.eps = (m == SMADFT_MODEL_QUASI ? -0.001 : -0.01) * std::atof(pos[1].c_str());
+    if (pos.size() >= 2) p.eps = (m >= SMADFT_MODEL_QUASI ? -0.001 : -0.01) * std::atof(pos[1].c_str());
     if (pos.size() >= 3) o.kv.emplace("radius", pos[2]);
     if (pos.size() >= 4 && std::atoi(pos[3].c_str()) == 1) {
         o.kv.emplace("ic", "file:psi0.dat");
@@ -95,15 +99,20 @@ int main(int argc, char **argv)
     p.alpha = o.num("alpha", p.alpha); p.beta = o.num("beta", p.beta); p.gamma = o.num("gamma", p.gamma);
     p.nu = o.num("nu", p.nu); p.kp = o.num("kp", p.kp); p.rho0 = o.num("rho0", p.rho0);
     p.divv_switch = (int)o.num("divv", p.divv_switch);
+    p.zeta = o.num("zeta", p.zeta);
+    p.rho_up = (int)o.num("rhoup", p.rho_up);
     p.precision = o.get("precision", "fp64") == "fp32" ? SMADFT_FP32 : SMADFT_FP64;
     p.conserved = (int)o.num("conserved", 0);
     const long steps = (long)o.num("steps", 1000);
-    const int l1every = (int)o.num("l1every", m == SMADFT_MODEL_QUASI ? 50 : 100);
+    const bool dens = m == SMADFT_MODEL_QUASI || m == SMADFT_MODEL_COMP;   // models with a density
+    const int l1every = (int)o.num("l1every", dens ? 50 : 100);
     const int saveevery = (int)o.num("saveevery", 10);
     const std::string out = o.get("out", ".") + "/";
     const int taxis = (int)o.num("track_axis", 2);
-    const int tmode = (int)o.num("track_mode", m == SMADFT_MODEL_QUASI ? SMADFT_TRACK_LEVEL : SMADFT_TRACK_FLAT);
-    const double thi = o.num("track_hi", m == SMADFT_MODEL_QUASI ? p.rho0 + 0.2 : 0.7);
+    const int tmode = (int)o.num("track_mode", dens ? SMADFT_TRACK_LEVEL : SMADFT_TRACK_FLAT);
+    // quasi: rho > rho_0 + 0.2 (quasi/quasi.cpp:2264-2280); comp: rho > rho_s - 0.15 with
+    // rho_s = 1 (compressible/compressible.cpp:2734)
+    const double thi = o.num("track_hi", m == SMADFT_MODEL_QUASI ? p.rho0 + 0.2 : m == SMADFT_MODEL_COMP ? 0.85 : 0.7);
     const double tlo = o.num("track_lo", 0.0);
     int rc = smadft_params_check(&p);
     if (rc) return die("parameter check", rc, nullptr);
@@ -137,10 +146,11 @@ int main(int argc, char **argv)
 
     {   // files are created empty, as the reference does at start-up
         for (const char *f : {"L1.dat", "psiMid.dat", "surfPsi.dat"}) std::ofstream(out + f).close();
-        if (m != SMADFT_MODEL_QUASI)
+        if (!dens)
             for (const char *f : {"velSurf.dat", "curvH.dat", "curvK.dat"}) std::ofstream(out + f).close();
         if (m != SMADFT_MODEL_NOADV) for (const char *f : {"vx.dat", "vy.dat", "vz.dat"}) std::ofstream(out + f).close();
-        if (m == SMADFT_MODEL_QUASI) for (const char *f : {"mass.dat", "energy.dat"}) std::ofstream(out + f).close();
+        if (dens) for (const char *f : {"mass.dat", "energy.dat"}) std::ofstream(out + f).close();
+        if (m == SMADFT_MODEL_COMP) for (const char *f : {"rhoMid.dat", "amp.dat"}) std::ofstream(out + f).close();
         std::ofstream info(out + "info");
         info << "Nx: " << p.nx << "\nNy: " << p.ny << "\nNz: " << p.nz << "\nPoints per wavelength (nw): "
              << p.nw << "\nq0 (z direction): " << p.q0 << "\nepsilon: " << p.eps << "\nbeta: " << p.beta
@@ -157,7 +167,7 @@ int main(int argc, char **argv)
     // the reference's own save iteration (z-scanning flat tracker, noadv / adv) also writes the
     // normal velocity and curvatures of that step (no-adv/cosNoAdvTrackSing.cpp:808-1021,
     // adv/cosAdvTrackMult.cpp:1311-1585)
-    const bool with_surface = m != SMADFT_MODEL_QUASI && !p.conserved && taxis == 2 && tmode == SMADFT_TRACK_FLAT;
+    const bool with_surface = !dens && !p.conserved && taxis == 2 && tmode == SMADFT_TRACK_FLAT;
     while (done < steps) {
         long chunk = std::min<long>(l1every - 1, steps - done - 1);
         if (chunk > 0 && (rc = smadft_step(ctx, (int)chunk))) return die("smadft_step", rc, ctx);
@@ -173,13 +183,13 @@ int main(int argc, char **argv)
         }
         if (rc) return die("smadft_step_diag", rc, ctx);
         std::ofstream(out + "L1.dat", std::ios_base::app) << std::setprecision(17) << d.l1 << "\n";
-        if (m == SMADFT_MODEL_QUASI) {
+        if (dens) {
             std::ofstream(out + "mass.dat", std::ios_base::app) << std::setprecision(17) << d.mass << "\n";
             std::ofstream(out + "energy.dat", std::ios_base::app) << std::setprecision(17) << d.energy << "\n";
         }
         if (++countSave == saveevery) {
             countSave = 0;
-            int fld = (m == SMADFT_MODEL_QUASI && tmode == SMADFT_TRACK_LEVEL) ? SMADFT_FIELD_RHO : SMADFT_FIELD_PSI;
+            int fld = (dens && tmode == SMADFT_TRACK_LEVEL) ? SMADFT_FIELD_RHO : SMADFT_FIELD_PSI;
             if (!surf_iter && (rc = smadft_track(ctx, fld, taxis, tmode, thi, tlo, sidx.data(), spos.data())))
                 return die("smadft_track", rc, ctx);
             {
@@ -197,6 +207,14 @@ int main(int argc, char **argv)
             }
             if ((rc = smadft_get_psi(ctx, field.data(), N))) return die("smadft_get_psi", rc, ctx);
             append_slice(out + "psiMid.dat", field, p.nx, p.ny, p.nz);
+            if (m == SMADFT_MODEL_COMP) {
+                int ids[2] = {SMADFT_FIELD_RHO, SMADFT_FIELD_AMP};
+                const char *names[2] = {"rhoMid.dat", "amp.dat"};
+                for (int c = 0; c < 2; c++) {
+                    if ((rc = smadft_get_field(ctx, ids[c], field.data(), N))) return die("smadft_get_field", rc, ctx);
+                    append_slice(out + names[c], field, p.nx, p.ny, p.nz);
+                }
+            }
             if (m != SMADFT_MODEL_NOADV) {
                 int ids[3] = {SMADFT_FIELD_VX, SMADFT_FIELD_VY, SMADFT_FIELD_VZ};
                 const char *names[3] = {"vx.dat", "vy.dat", "vz.dat"};
@@ -213,6 +231,12 @@ int main(int argc, char **argv)
     if ((rc = smadft_get_psi(ctx, psi.data(), N))) return die("smadft_get_psi", rc, ctx);
     {
         std::ofstream s(out + "psi0.dat");
+        s << std::setprecision(17);
+        for (size_t q = 0; q < N; q++) s << psi[q] << "\n";
+    }
+    if (m == SMADFT_MODEL_COMP) {   // the density save beside psi (compressible/compressible.cpp:2786-2799)
+        if ((rc = smadft_get_field(ctx, SMADFT_FIELD_RHO, psi.data(), N))) return die("smadft_get_field", rc, ctx);
+        std::ofstream s(out + "rho0.dat");
         s << std::setprecision(17);
         for (size_t q = 0; q < N; q++) s << psi[q] << "\n";
     }

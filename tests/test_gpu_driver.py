@@ -96,3 +96,31 @@ def test_driver_conserved_run_matches_oracle(tmp_path, model, omodel, extra):
     assert read(tmp_path / "velSurf.dat").size == 0      # no conserved surface diagnostics
     final = read(tmp_path / "psi0.dat").reshape(shape)
     assert np.max(np.abs(final - o.get(oracle.F_PSI))) <= 1e-10 * np.max(np.abs(final))
+
+
+def test_driver_comp_run_matches_oracle(tmp_path):
+    if not os.path.exists(DRIVER):
+        pytest.skip("smadft_run not built")
+    shape = (16, 12, 20)
+    x = np.arange(shape[0])[:, None, None]
+    z = np.arange(shape[2])[None, None, :] * 2 * np.pi / 8
+    psi0 = 1.3 * np.cos(z) * 0.5 * (1 - np.tanh((x - 8) / 4.0)) * np.ones((1, shape[1], 1))
+    ic = tmp_path / "ic.txt"
+    np.savetxt(ic, psi0.reshape(-1), fmt="%.17g")
+    args = [DRIVER, "comp", f"nx={shape[0]}", f"ny={shape[1]}", f"nz={shape[2]}", "nw=8", "eps=-0.75",
+            "dt=0.001", "divv=30", "rhoup=4", "steps=100", "l1every=50", "saveevery=2", f"ic=file:{ic}",
+            f"out={tmp_path}"]
+    subprocess.run(args, check=True, capture_output=True, text=True)
+    o = oracle.Oracle(oracle.COMP, shape, nw=8, eps=-0.75, dt=0.001, nu=1.0, rho0=0.01, zeta=0.001,
+                      divv_switch=30, rho_up=4)
+    o.set_psi(psi0)
+    want = []
+    for _ in range(2):
+        o.step(50)
+        want.append(o.diag())
+    for name, key in (("L1.dat", "l1"), ("mass.dat", "mass"), ("energy.dat", "energy")):
+        assert np.allclose(read(tmp_path / name), [w[key] for w in want], rtol=1e-10, atol=0), name
+    assert np.max(np.abs(read(tmp_path / "rho0.dat").reshape(shape) - o.get(oracle.F_RHO))) <= 1e-10
+    final = read(tmp_path / "psi0.dat").reshape(shape)
+    assert np.max(np.abs(final - o.get(oracle.F_PSI))) <= 1e-10 * np.max(np.abs(final))
+    assert read(tmp_path / "amp.dat").size == shape[0] * shape[2]
