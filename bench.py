@@ -526,6 +526,7 @@ def run_kernel_only(args):
     pass-z | pass-y | pass-x: one plain DCT-II axis pass on a 256^3 field (2 fields held).
     r2r3d: one plain 3-D DCT-III (the plane kernel for z and y where it applies, then x).
     step: loop bodies of the adv model (all its kernels).
+    comp-step: loop bodies of the compressible model past its relaxation switch.
     """
     import torch
     import smadft
@@ -548,11 +549,20 @@ def run_kernel_only(args):
             torch.cuda.synchronize()
             for _ in range(args.reps):
                 s.r2r3d_device(x.data_ptr(), y.data_ptr(), (1, 1, 1))
-        else:
+        elif args.kernel_only == "step":
             p2 = smadft.params(smadft.ADV, (n, n, n), **CFG)
             s.set_psi(smadft.ic_conics(p2, A=1.328, count=4, rmin=3.0, rmax=6.0, seed=1))
             s.step(args.reps)
         s.sync()
+    if args.kernel_only == "comp-step":
+        pc = smadft.params(smadft.COMP, (n, n, n), precision=prec, divv_switch=1)
+        x = np.arange(n)[:, None, None]
+        z = np.arange(n)[None, None, :] * 2 * np.pi / 8
+        with smadft.Solver(pc) as s:
+            s.set_psi(1.3 * np.cos(z) * 0.5 * (1 - np.tanh((x - n / 2) / 4.0)) * np.ones((1, n, 1)))
+            s.step(1)
+            s.step(args.reps)
+            s.sync()
     print(f"kernel-only {args.kernel_only} {n}^3 {args.precision} x{args.reps}: done")
     return 0
 
@@ -567,7 +577,7 @@ def main():
                     help="steps of the 48-run batched sweep (config 4 runs 2000; 0: skip)")
     ap.add_argument("--err-steps", type=int, default=ERR_STEPS,
                     help="steps after which the FP32 error against FP64 is reported (0: after the timed steps)")
-    ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "r2r3d", "step"], default=None,
+    ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "r2r3d", "step", "comp-step"], default=None,
                     help="launch one kernel family a few times (for profilers) and exit")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--adjoint-steps", type=int, default=500,

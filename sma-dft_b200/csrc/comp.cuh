@@ -105,71 +105,76 @@ struct LdCForce {
 // Solenoidal and irrotational velocity spectra (:1838-2410), one thread per mode:
 //   vsol_x = CM1x/nu (Sx - CM2x dot),  virr_x = CM1x/(lambda + 2 nu) (s_i fgrad'[i+1] + CM2x dot G)
 // with CM1 = scale/|q_s|^2, CM2 = s/|q_s|^2, dot the shifted-neighbour product of LdStokes,
-// fgrad' = fgrad + e exp(-2 1.57^2 q^2) and G = exp(-2 1.57^2 |q_s|^2).  v_x for i < nx-1,
-// v_y, v_z for j < ny-1 and k < nz-1 (zero elsewhere).  The reference's k = 0 branch of v_z
-// for i >= 1, 0 < j < ny-1 takes G from CM1y (:2348-2350); so does this kernel.
+// fgrad' = fgrad + e exp(-2 1.57^2 q^2) and G = exp(-2 1.57^2 |q_s|^2), both from the
+// per-axis factor tables.  v_x for i < nx-1, v_y, v_z for j < ny-1 and k < nz-1 (zero
+// elsewhere).  The reference's k = 0 branch of v_z for i >= 1, 0 < j < ny-1 takes G from
+// CM1y (:2348-2350); so does this kernel.  Grid: x = k blocks, y = j, z = i.
 template <typename T>
 __global__ void comp_vel_kernel(Spec<T> s, const T *__restrict__ Sx, const T *__restrict__ Sy, const T *__restrict__ Sz,
                                 const T *__restrict__ fg, const T *__restrict__ en, T *__restrict__ vsx,
                                 T *__restrict__ vsy, T *__restrict__ vsz, T *__restrict__ vix, T *__restrict__ viy,
-                                T *__restrict__ viz, long long n)
+                                T *__restrict__ viz)
 {
-    const T sc = s.scale, l2n = s.lam + T(2) * s.nu, gk = T(-1.57 * 1.57 * 2);
-    const long long nyz = s.nyz;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(q % s.nz), j = (int)((q / s.nz) % s.ny), i = (int)(q / nyz);
-        const T qi = s.qx[i], qj = s.qy[j], qk = s.qz[k], si = s.sx[i], sj = s.sy[j], sk = s.sz[k];
-        T vx = T(0), ix = T(0), vy = T(0), iy = T(0), vz = T(0), iz = T(0);
-        if (i < s.nx - 1) {
-            const T syv = j != 0 ? Sy[q + nyz - s.nz] : T(0);    // (i+1, j-1, k)
-            const T szv = k != 0 ? Sz[q + nyz - 1] : T(0);       // (i+1, j, k-1)
-            const T m2 = si * si + qj * qj + qk * qk, cm1 = sc / m2, cm2 = si / m2;
-            const T dot = si * Sx[q] + qj * syv + qk * szv;
-            const T fgn = fg[q + nyz] + en[q + nyz] * (s.ex[i + 1] * s.ey[j] * s.ez[k]);
-            vx = (cm1 / s.nu) * (Sx[q] - cm2 * dot);
-            ix = (cm1 / l2n) * (si * fgn + cm2 * dot * exp(gk * m2));
-        }
-        if (j < s.ny - 1 && k < s.nz - 1) {
-            T sxv = i != 0 ? Sx[q - nyz + s.nz] : T(0);           // (i-1, j+1, k)
-            const T szv = k != 0 ? Sz[q + s.nz - 1] : T(0);       // (i, j+1, k-1)
-            const T m2y = qi * qi + sj * sj + qk * qk;
-            T cm1 = sc / m2y, cm2 = sj / m2y;
-            T dot = qi * sxv + sj * Sy[q] + qk * szv;
-            const T fgy = fg[q + s.nz] + en[q + s.nz] * (s.ex[i] * s.ey[j + 1] * s.ez[k]);
-            vy = (cm1 / s.nu) * (Sy[q] - cm2 * dot);
-            iy = (cm1 / l2n) * (sj * fgy + cm2 * dot * exp(gk * m2y));
-            sxv = i != 0 ? Sx[q - nyz + 1] : T(0);                // (i-1, j, k+1)
-            const T syv = j != 0 ? Sy[q - s.nz + 1] : T(0);       // (i, j-1, k+1)
-            const T m2z = qi * qi + qj * qj + sk * sk;
-            cm1 = sc / m2z;
-            cm2 = sk / m2z;
-            dot = qi * sxv + qj * syv + sk * Sz[q];
-            const T fgz = fg[q + 1] + en[q + 1] * (s.ex[i] * s.ey[j] * s.ez[k + 1]);
-            const T mf = (i >= 1 && k == 0 && j >= 1) ? m2y : m2z;
-            vz = (cm1 / s.nu) * (Sz[q] - cm2 * dot);
-            iz = (cm1 / l2n) * (sk * fgz + cm2 * dot * exp(gk * mf));
-        }
-        vsx[q] = vx; vsy[q] = vy; vsz[q] = vz;
-        vix[q] = ix; viy[q] = iy; viz[q] = iz;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, i = blockIdx.z;
+    if (k >= s.nz) return;
+    const idx_t nyz = s.nyz, nz = s.nz;
+    const idx_t q = (idx_t)i * nyz + (idx_t)j * nz + k;
+    // one reciprocal per component: CM1 = scale/m2, CM2 = s/m2; 1/nu and 1/(lambda + 2 nu) hoisted
+    const T sc = s.scale, inu = T(1) / s.nu, il2n = T(1) / (s.lam + T(2) * s.nu);
+    const T qi = s.qx[i], qj = s.qy[j], qk = s.qz[k], si = s.sx[i], sj = s.sy[j], sk = s.sz[k];
+    const T exi = s.ex[i], eyj = s.ey[j], ezk = s.ez[k];
+    T vx = T(0), ix = T(0), vy = T(0), iy = T(0), vz = T(0), iz = T(0);
+    if (i < s.nx - 1) {
+        const T syv = j != 0 ? Sy[q + nyz - nz] : T(0);    // (i+1, j-1, k)
+        const T szv = k != 0 ? Sz[q + nyz - 1] : T(0);     // (i+1, j, k-1)
+        const T inv = T(1) / (si * si + qj * qj + qk * qk), cm1 = sc * inv, cm2 = si * inv;
+        const T dot = si * Sx[q] + qj * syv + qk * szv;
+        const T fgn = fg[q + nyz] + en[q + nyz] * (s.ex[i + 1] * eyj * ezk);
+        vx = (cm1 * inu) * (Sx[q] - cm2 * dot);
+        ix = (cm1 * il2n) * (si * fgn + cm2 * dot * (s.esx[i] * eyj * ezk));
     }
+    if (j < s.ny - 1 && k < s.nz - 1) {
+        T sxv = i != 0 ? Sx[q - nyz + nz] : T(0);            // (i-1, j+1, k)
+        const T szv = k != 0 ? Sz[q + nz - 1] : T(0);        // (i, j+1, k-1)
+        const T invy = T(1) / (qi * qi + sj * sj + qk * qk);
+        T cm1 = sc * invy, cm2 = sj * invy;
+        T dot = qi * sxv + sj * Sy[q] + qk * szv;
+        const T gy = exi * s.esy[j] * ezk;
+        const T fgy = fg[q + nz] + en[q + nz] * (exi * s.ey[j + 1] * ezk);
+        vy = (cm1 * inu) * (Sy[q] - cm2 * dot);
+        iy = (cm1 * il2n) * (sj * fgy + cm2 * dot * gy);
+        sxv = i != 0 ? Sx[q - nyz + 1] : T(0);               // (i-1, j, k+1)
+        const T syv = j != 0 ? Sy[q - nz + 1] : T(0);        // (i, j-1, k+1)
+        const T invz = T(1) / (qi * qi + qj * qj + sk * sk);
+        cm1 = sc * invz;
+        cm2 = sk * invz;
+        dot = qi * sxv + qj * syv + sk * Sz[q];
+        const T fgz = fg[q + 1] + en[q + 1] * (exi * eyj * s.ez[k + 1]);
+        const T gz = (i >= 1 && k == 0 && j >= 1) ? gy : exi * eyj * s.esz[k];
+        vz = (cm1 * inu) * (Sz[q] - cm2 * dot);
+        iz = (cm1 * il2n) * (sk * fgz + cm2 * dot * gz);
+    }
+    vsx[q] = vx; vsy[q] = vy; vsz[q] = vz;
+    vix[q] = ix; viy[q] = iy; viz[q] = iz;
 }
 
 // div v and the penalty-force divergence from the shifted spectra (:2478-2527):
 //   divv = q . virr[-1 shifts],  ampd = scale q . f[-1 shifts]  (index -1 -> 0)
+// Grid as comp_vel_kernel.
 template <typename T>
 __global__ void comp_div_kernel(Spec<T> s, const T *__restrict__ vix, const T *__restrict__ viy, const T *__restrict__ viz,
                                 const T *__restrict__ fx, const T *__restrict__ fy, const T *__restrict__ fz,
-                                T *__restrict__ dv, T *__restrict__ ad, long long n)
+                                T *__restrict__ dv, T *__restrict__ ad)
 {
-    const long long nyz = s.nyz;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(q % s.nz), j = (int)((q / s.nz) % s.ny), i = (int)(q / nyz);
-        const T a = i > 0 ? vix[q - nyz] : T(0), fa = i > 0 ? fx[q - nyz] : T(0);
-        const T b = j > 0 ? viy[q - s.nz] : T(0), fb = j > 0 ? fy[q - s.nz] : T(0);
-        const T c = k > 0 ? viz[q - 1] : T(0), fc = k > 0 ? fz[q - 1] : T(0);
-        dv[q] = s.qx[i] * a + s.qy[j] * b + s.qz[k] * c;
-        ad[q] = s.scale * (s.qx[i] * fa + s.qy[j] * fb + s.qz[k] * fc);
-    }
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, i = blockIdx.z;
+    if (k >= s.nz) return;
+    const idx_t nyz = s.nyz, nz = s.nz;
+    const idx_t q = (idx_t)i * nyz + (idx_t)j * nz + k;
+    const T a = i > 0 ? vix[q - nyz] : T(0), fa = i > 0 ? fx[q - nyz] : T(0);
+    const T b = j > 0 ? viy[q - nz] : T(0), fb = j > 0 ? fy[q - nz] : T(0);
+    const T c = k > 0 ? viz[q - 1] : T(0), fc = k > 0 ? fz[q - 1] : T(0);
+    dv[q] = s.qx[i] * a + s.qy[j] * b + s.qz[k] * c;
+    ad[q] = s.scale * (s.qx[i] * fa + s.qy[j] * fb + s.qz[k] * fc);
 }
 
 // Mass balance, AB2 in real space (:2555-2573):
@@ -321,9 +326,12 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
             return rc;
     }
     // velocity spectra, div v and the penalty divergence (:1826-2527)
-    comp_vel_kernel<T><<<c.red_blocks, 256, 0, c.stream>>>(s, Sx, Sy, Sz, fg, en, vsx, vsy, vsz, vix, viy, viz, n);
-    SMADFT_CUDA(cudaGetLastError());
-    comp_div_kernel<T><<<c.red_blocks, 256, 0, c.stream>>>(s, vix, viy, viz, fx, fy, fz, dv, ad, n);
+    {
+        const dim3 blk(128), grd((unsigned)((c.g.nz + 127) / 128), (unsigned)c.g.ny, (unsigned)c.g.nx);
+        comp_vel_kernel<T><<<grd, blk, 0, c.stream>>>(s, Sx, Sy, Sz, fg, en, vsx, vsy, vsz, vix, viy, viz);
+        SMADFT_CUDA(cudaGetLastError());
+        comp_div_kernel<T><<<grd, blk, 0, c.stream>>>(s, vix, viy, viz, fx, fy, fz, dv, ad);
+    }
     SMADFT_CUDA(cudaGetLastError());
     c.launches += 2;
     // all eight back to real space, in place (:2521-2552): one grouped launch for the y passes

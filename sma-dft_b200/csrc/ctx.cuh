@@ -50,6 +50,7 @@ template <typename T>
 struct Spec {
     const T *qx, *qy, *qz, *sx, *sy, *sz;   // DCT / DST wavenumbers per axis
     const T *ex, *ey, *ez;                   // exp(-2 * 1.57^2 q^2) per axis (quasi filter)
+    const T *esx, *esy, *esz;                // exp(-2 * 1.57^2 s^2) per axis (DST wavenumbers)
     T eps, alpha, beta, gamma, q02, dtd2, dt, scale, nu;
     T rho_m, lam, kp, rho0;
     T zeta, amp0;                            // compressible: density penalty, one-mode amplitude
@@ -78,10 +79,10 @@ struct Ctx {
     std::string err;
     void *slot[S_COUNT] = {};
     size_t esize = 8;
-    void *tables = nullptr;     // qx qy qz sx sy sz ex ey ez (T), contiguous
-    size_t off[9] = {};
+    void *tables = nullptr;     // qx qy qz sx sy sz ex ey ez esx esy esz (T), contiguous
+    size_t off[12] = {};
     void *tables64 = nullptr;   // the same in FP64 (= tables for FP64 contexts): time-update coefficients
-    size_t off64[9] = {};
+    size_t off64[12] = {};
     std::map<int, PlanDev> plans;
     double *red = nullptr;      // reduction partials (device)
     double *red_out = nullptr;  // final sums (device)
@@ -128,10 +129,12 @@ Spec<T> make_spec(const Ctx &c)
         auto t = [&](int w) { return reinterpret_cast<const T *>(reinterpret_cast<const char *>(c.tables64) + c.off64[w]); };
         s.qx = t(0); s.qy = t(1); s.qz = t(2); s.sx = t(3); s.sy = t(4); s.sz = t(5);
         s.ex = t(6); s.ey = t(7); s.ez = t(8);
+        s.esx = t(9); s.esy = t(10); s.esz = t(11);
     } else {
         s.qx = c.tab<T>(0); s.qy = c.tab<T>(1); s.qz = c.tab<T>(2);
         s.sx = c.tab<T>(3); s.sy = c.tab<T>(4); s.sz = c.tab<T>(5);
         s.ex = c.tab<T>(6); s.ey = c.tab<T>(7); s.ez = c.tab<T>(8);
+        s.esx = c.tab<T>(9); s.esy = c.tab<T>(10); s.esz = c.tab<T>(11);
     }
     const smadft_params &p = c.p;
     s.eps = T(p.eps); s.alpha = T(p.alpha); s.beta = T(p.beta); s.gamma = T(p.gamma);

@@ -90,6 +90,7 @@ int upload_tables(Ctx &c)
 {
     const int nx = c.g.nx, ny = c.g.ny, nz = c.g.nz;
     std::vector<double> qx(nx), qy(ny), qz(nz), sx(nx), sy(ny), sz(nz), ex(nx), ey(ny), ez(nz);
+    std::vector<double> esx(nx), esy(ny), esz(nz);
     for (int i = 0; i < nx; i++) { qx[i] = 1.0 * M_PI * i / (c.dx * nx); sx[i] = 1.0 * M_PI * (i + 1) / (c.dx * nx); }
     for (int j = 0; j < ny; j++) { qy[j] = M_PI * (j) / (c.dy * ny); sy[j] = M_PI * (j + 1) / (c.dy * ny); }
     for (int k = 0; k < nz; k++) { qz[k] = M_PI * (k) / (c.dz * nz); sz[k] = M_PI * (k + 1) / (c.dz * nz); }
@@ -98,9 +99,14 @@ int upload_tables(Ctx &c)
     for (int i = 0; i < nx; i++) ex[i] = std::exp(-fk * qx[i] * qx[i]);
     for (int j = 0; j < ny; j++) ey[j] = std::exp(-fk * qy[j] * qy[j]);
     for (int k = 0; k < nz; k++) ez[k] = std::exp(-fk * qz[k] * qz[k]);
-    const std::vector<double> *t[9] = {&qx, &qy, &qz, &sx, &sy, &sz, &ex, &ey, &ez};
+    // the same factor on the DST wavenumbers: the compressible model's irrotational-velocity
+    // filter exp(-2 1.57^2 |q_s|^2) (compressible/compressible.cpp:1985), separable per axis
+    for (int i = 0; i < nx; i++) esx[i] = std::exp(-fk * sx[i] * sx[i]);
+    for (int j = 0; j < ny; j++) esy[j] = std::exp(-fk * sy[j] * sy[j]);
+    for (int k = 0; k < nz; k++) esz[k] = std::exp(-fk * sz[k] * sz[k]);
+    const std::vector<double> *t[12] = {&qx, &qy, &qz, &sx, &sy, &sz, &ex, &ey, &ez, &esx, &esy, &esz};
     std::vector<T> all;
-    for (int q = 0; q < 9; q++) {
+    for (int q = 0; q < 12; q++) {
         c.off[q] = all.size() * sizeof(T);
         for (double v : *t[q]) all.push_back(T(v));
     }
@@ -108,10 +114,10 @@ int upload_tables(Ctx &c)
     SMADFT_CUDA(cudaMemcpy(c.tables, all.data(), all.size() * sizeof(T), cudaMemcpyHostToDevice));
     if (sizeof(T) == 8) {
         c.tables64 = c.tables;
-        for (int q = 0; q < 9; q++) c.off64[q] = c.off[q];
+        for (int q = 0; q < 12; q++) c.off64[q] = c.off[q];
     } else {
         std::vector<double> all64;
-        for (int q = 0; q < 9; q++) {
+        for (int q = 0; q < 12; q++) {
             c.off64[q] = all64.size() * sizeof(double);
             for (double v : *t[q]) all64.push_back(v);
         }
