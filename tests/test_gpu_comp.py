@@ -104,3 +104,43 @@ def test_comp_has_no_surface_output_or_adjoint():
         with pytest.raises(smadft.SmadftError) as e:
             s.adjoint(4, checkpoint_every=2)
         assert e.value.code == -6
+
+
+def test_batch_with_comp_members_matches_solo_runs():
+    cases = [make((16, 12, 20), divv_switch=3, rho_up=4), make((24, 64, 64), precision=smadft.FP32, divv_switch=2),
+             smadft.params(smadft.ADV, (16, 64, 64), dt=0.01)]
+    solo = []
+    for i, p in enumerate(cases):
+        with smadft.Solver(p) as s:
+            s.set_psi(ic((p.nx, p.ny, p.nz), seed=30 + i))
+            s.step(5)
+            solo.append(s.get("psi"))
+    with smadft.Batch(cases) as b:
+        for i, p in enumerate(cases):
+            b.members[i].set_psi(ic((p.nx, p.ny, p.nz), seed=30 + i))
+        b.step(2)
+        b.step(3)
+        b.sync()
+        for i in range(len(cases)):
+            assert np.array_equal(b.members[i].get("psi"), solo[i]), i
+
+
+def test_autotune_keeps_a_comp_run():
+    # ny = nz = 64 offers the fused plane path too; the in-place inverse group then goes
+    # through the scratch field
+    shape = (16, 64, 64)
+    p = make(shape, divv_switch=2, rho_up=4)
+    psi0 = ic(shape, seed=9)
+    with smadft.Solver(p) as a:
+        a.set_psi(psi0)
+        a.step(3)
+        rep = a.autotune(2)
+        a.step(4)
+        got = a.get("psi"), a.get("rho")
+    with smadft.Solver(p) as b:
+        b.set_psi(psi0)
+        b.step(7)
+        want = b.get("psi"), b.get("rho")
+    assert rep["chosen"] in rep["ms_per_step"] and len(rep["ms_per_step"]) >= 4
+    for g, w in zip(got, want):
+        assert np.max(np.abs(g - w)) <= 1e-11 * np.max(np.abs(w))
