@@ -2,6 +2,7 @@
 // diagnostics, interface tracker and checkpoints.  See include/smadft.h for the contract.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
@@ -426,8 +427,14 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
         if (cudaEventCreateWithFlags(&c.ev_join[m], cudaEventDisableTiming) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
     }
     if (cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+    // Host-side fault injection for the failure tests: SMADFT_FAIL_ALLOC=k makes the k-th
+    // field allocation of this call report out-of-memory (nothing is allocated for it), so
+    // the clean-up path runs without a real allocation failure.
+    int fail_at = -1, nalloc = 0;
+    if (const char *e = std::getenv("SMADFT_FAIL_ALLOC")) fail_at = std::atoi(e);
     for (int s : slots_for(p->model)) {
         const size_t bytes = (slot_is_state(s) ? sizeof(double) : c.esize) * c.n;
+        if (nalloc++ == fail_at) return bail(SMADFT_ERR_NOMEM);
         if (cudaMalloc(&c.slot[s], bytes) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
         if (cudaMemset(c.slot[s], 0, bytes) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
     }
