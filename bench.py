@@ -172,6 +172,27 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+def max_over_ranks(torch, dist, values, device):
+    """Element-wise maximum of a list of floats over all ranks (one all-reduce on `device`:
+    "cuda" under NCCL, "cpu" under gloo)."""
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def partition_by_cost(costs, world: int, rank: int):
+    """Indices of the runs rank `rank` takes: greedy, largest cost first, each to the least
+    loaded rank (no collective; every rank computes the same split)."""
+    load = [0.0] * world
+    mine = []
+    for idx in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        r = min(range(world), key=lambda w: (load[w], w))
+        load[r] += costs[idx]
+        if r == rank:
+            mine.append(idx)
+    return sorted(mine)
+
+
 def timed_steps(torch, solver, steps: int, dist, world, sampler=None):
     """Device time of `steps` loop bodies on the solver's stream, max over ranks."""
     stream = torch.cuda.ExternalStream(solver.stream)
@@ -190,9 +211,7 @@ def timed_steps(torch, solver, steps: int, dist, world, sampler=None):
     ms = ev0.elapsed_time(ev1)
     launches = solver.launches - l0
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(torch, dist, [ms], "cuda")[0]
         dist.barrier()
     return ms, launches
 
@@ -264,13 +283,7 @@ def run_batch_sweep(torch, smadft, steps, rank, world, dist):
     N^3 F, F = 6 noadv / 32 adv), each autotuned, then `steps` batch steps timed with CUDA
     events on the batch; the same runs stepped one context after another for comparison."""
     runs = sweep_params(smadft)
-    load = [0.0] * world
-    mine = []
-    for idx in sorted(range(len(runs)), key=lambda i: -runs[i][1] ** 3 * (6 if runs[i][0] == smadft.NOADV else 32)):
-        r = min(range(world), key=lambda w: load[w])
-        load[r] += runs[idx][1] ** 3 * (6 if runs[idx][0] == smadft.NOADV else 32)
-        if r == rank:
-            mine.append(idx)
+    mine = partition_by_cost([n ** 3 * (6 if model == smadft.NOADV else 32) for model, n, _, _ in runs], world, rank)
     plist = []
     for i in sorted(mine):
         model, n, kw, _ = runs[i]
@@ -307,9 +320,7 @@ def run_batch_sweep(torch, smadft, steps, rank, world, dist):
             m.sync()
         ms_solo = 1000.0 * (time.perf_counter() - t0)
     if world > 1:
-        t = torch.tensor([ms_batch, ms_solo], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_batch, ms_solo = float(t[0]), float(t[1])
+        ms_batch, ms_solo = max_over_ranks(torch, dist, [ms_batch, ms_solo], "cuda")
         c = torch.tensor([float(finite)], device="cuda")
         dist.all_reduce(c, op=dist.ReduceOp.MIN)
         finite = bool(c.item())
@@ -460,9 +471,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         e2e_ms = ev0.elapsed_time(ev1)
         if world > 1:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+            e2e_ms = max_over_ranks(torch, dist, [e2e_ms], "cuda")[0]
     e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
 
     sweep = run_batch_sweep(torch, smadft, args.sweep_steps, rank, world, dist) if args.sweep_steps > 0 else None
