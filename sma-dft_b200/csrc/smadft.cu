@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "ctx.cuh"
 #include "reduce.cuh"
 #include "smadft.h"
@@ -32,6 +34,15 @@ struct smadft_ctx {
     std::map<int, StepGraph> graphs;
     bool use_graphs = true;
     SurfaceScratch surf;
+};
+
+// One NVTX range per ABI call, named after the call: profilers (nsys, ncu --nvtx) group the
+// call's kernels under it; without a tool attached a range costs a few nanoseconds.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
 };
 
 namespace {
@@ -489,6 +500,7 @@ const char *smadft_last_error(const smadft_ctx *h)
 
 int smadft_set_psi(smadft_ctx *h, const double *host, size_t n)
 {
+    NvtxRange nvtx_("smadft_set_psi");
     if (!h || !host) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if ((long long)n != c.n) return fail(c, SMADFT_ERR_INVALID, "size mismatch");
@@ -584,6 +596,7 @@ static int graph_step(smadft_ctx *h)
 
 int smadft_step(smadft_ctx *h, int nsteps)
 {
+    NvtxRange nvtx_("smadft_step");
     if (!h || nsteps < 0) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
@@ -599,6 +612,7 @@ int smadft_step(smadft_ctx *h, int nsteps)
 
 int smadft_step_diag(smadft_ctx *h, smadft_diag *out)
 {
+    NvtxRange nvtx_("smadft_step_diag");
     if (!h || !out) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
@@ -610,6 +624,7 @@ int smadft_step_diag(smadft_ctx *h, smadft_diag *out)
 int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH, double *curvK,
                         smadft_diag *diag)
 {
+    NvtxRange nvtx_("smadft_step_surface");
     if (!h || !surf_idx || !vel || !curvH || !curvK) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if (!c.have_psi) return fail(c, SMADFT_ERR_STATE, "no initial condition");
@@ -645,6 +660,7 @@ int smadft_step_surface(smadft_ctx *h, int *surf_idx, double *vel, double *curvH
 
 int smadft_adjoint(smadft_ctx *h, const smadft_adj_opts *o, smadft_grads *out, double *d_psi0)
 {
+    NvtxRange nvtx_("smadft_adjoint");
     if (!h || !o || !out || o->steps <= 0 || o->checkpoint_every <= 0 || o->axis < 0 || o->axis > 2 ||
         (o->mode != SMADFT_TRACK_FLAT && o->mode != SMADFT_TRACK_BUMP))
         return SMADFT_ERR_INVALID;
@@ -697,6 +713,7 @@ int smadft_free_energy(smadft_ctx *h, double *out)
 
 int smadft_step_host(smadft_ctx *h, double *host, size_t n, int nsteps)
 {
+    NvtxRange nvtx_("smadft_step_host");
     if (!h || !host || nsteps < 0) return SMADFT_ERR_INVALID;
     Ctx &c = h->c;
     if ((long long)n != c.n) return fail(c, SMADFT_ERR_INVALID, "size mismatch");
