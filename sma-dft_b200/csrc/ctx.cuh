@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <type_traits>
 #include <string>
 #include <vector>
@@ -23,6 +24,14 @@ namespace smadft {
 // Kernel attributes (dynamic shared memory opt-in) are per device: launch helpers keep one
 // flag per device index below this bound.
 constexpr int kMaxDevices = 64;
+// Distinct contexts may be driven from different host threads: the per-device attribute
+// flags below are read and set under this lock (set once per kernel and device, so the lock
+// is taken while a step graph is captured, not in the replayed steps).
+inline std::mutex &attr_mutex()
+{
+    static std::mutex m;
+    return m;
+}
 
 // Field slots (allocated per model; unused slots stay null).
 enum Slot : int {
@@ -185,10 +194,13 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
     }
     const size_t smem = 2 * (size_t)(a.W / 2) * a.ld * sizeof(cpx<T>);
     static size_t attr_set[kMaxDevices] = {};   // largest opt-in so far, per device and instantiation
-    if (smem > attr_set[c.dev % kMaxDevices]) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_pass_kernel<T, LD, ST>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set[c.dev % kMaxDevices] = smem;
+    {
+        std::lock_guard<std::mutex> lock(attr_mutex());
+        if (smem > attr_set[c.dev % kMaxDevices]) {
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_pass_kernel<T, LD, ST>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set[c.dev % kMaxDevices] = smem;
+        }
     }
     r2r_pass_kernel<T, LD, ST><<<(unsigned)tiles, 256, smem, c.stream>>>(a, ld, st);
     SMADFT_CUDA(cudaGetLastError());
@@ -204,10 +216,13 @@ int launch_rd(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
     const long long tiles = (long long)(AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b * NC;
     constexpr size_t smem = rd_smem_bytes<T, N>();
     static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
-    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set |= 1ull << (c.dev % kMaxDevices);
+    {
+        std::lock_guard<std::mutex> lock(attr_mutex());
+        if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set |= 1ull << (c.dev % kMaxDevices);
+        }
     }
     r2r_rd_kernel<T, N, AXIS, LD, ST, NC><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         c.g, kinds, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
@@ -236,10 +251,13 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
     }
     constexpr size_t smem = fast_smem_bytes<T, N, CFG>();
     static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
-    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_fast_kernel<T, N, AXIS, LD, ST, CFG>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set |= 1ull << (c.dev % kMaxDevices);
+    {
+        std::lock_guard<std::mutex> lock(attr_mutex());
+        if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_fast_kernel<T, N, AXIS, LD, ST, CFG>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set |= 1ull << (c.dev % kMaxDevices);
+        }
     }
     r2r_fast_kernel<T, N, AXIS, LD, ST, CFG><<<(unsigned)tiles, CFG::THREADS, smem, c.stream>>>(
         c.g, kind, tiles_b, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), ld, st);
@@ -257,9 +275,12 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
     const int tiles = (rows + 2 * kRdLines - 1) / (2 * kRdLines);
     constexpr size_t smem = rdz_smem_bytes<T, N>();
     static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
-    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set |= 1ull << (c.dev % kMaxDevices);
+    {
+        std::lock_guard<std::mutex> lock(attr_mutex());
+        if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set |= 1ull << (c.dev % kMaxDevices);
+        }
     }
     r2r_rdz_kernel<T, N><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h));
@@ -350,10 +371,13 @@ int launch_plane(Ctx &c, const PlaneKinds<NC> &kinds, LD ld, const StoreMulti<T,
     constexpr size_t smem = plane_smem_bytes<T, N>();
     using ST = StoreMulti<T, NC>;
     static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
-    if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-        SMADFT_CUDA(cudaFuncSetAttribute(r2r_plane_kernel<T, N, NC, LD, ST>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set |= 1ull << (c.dev % kMaxDevices);
+    {
+        std::lock_guard<std::mutex> lock(attr_mutex());
+        if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_plane_kernel<T, N, NC, LD, ST>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set |= 1ull << (c.dev % kMaxDevices);
+        }
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)c.g.nx * NC * PlaneInfo<N>::C);
