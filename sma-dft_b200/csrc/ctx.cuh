@@ -106,6 +106,7 @@ struct Ctx {
     bool use_multi = true;      // one y-pass launch for the components of r2r3d_multi (SMADFT_MULTI=0: off)
     bool use_fork = true;       // independent per-component passes on forked streams (SMADFT_FORK=0: off)
     bool use_plane = false;
+    bool rdz_rev = true;        // z passes walk their tiles from the last row down (SMADFT_RDZ_REV=0: up)
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -283,7 +284,8 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
         }
     }
     r2r_rdz_kernel<T, N><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
-        rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h));
+        rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h),
+        c.rdz_rev ? 1 : 0);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
     return SMADFT_OK;

@@ -22,11 +22,14 @@ namespace smadft {
 template <typename T, int N>
 constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * sizeof(cpx<T>); }
 
-// rows = number of z lines (nx * ny); a CTA transforms 2 * kRdLines consecutive rows
+// rows = number of z lines (nx * ny); a CTA transforms 2 * kRdLines consecutive rows.
+// rev = 1 walks the tiles from the last row down: the pass before a z pass (the y pass of the
+// same transform) writes its field from x = 0 up, so the rows it wrote last, still in L2,
+// are read first.  Tiles are independent, so the order does not change the result.
 template <typename T, int N>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind, const T *in, T *out,
                                                                         const cpx<T> *__restrict__ wt_g,
-                                                                        const cpx<T> *__restrict__ ht_g)
+                                                                        const cpx<T> *__restrict__ ht_g, int rev)
 {
     using RI = RdInfo<N>;
     constexpr int R0 = RI::R0, R1 = RI::R1, NT = RI::THREADS;
@@ -44,7 +47,8 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     }
     const int j = threadIdx.x % R1;                 // first-stage butterfly (lane in its group)
     const int c = threadIdx.x / R1;                 // complex line of the CTA
-    const int ra = (int)blockIdx.x * (2 * kRdLines) + 2 * c;   // real rows ra, ra + 1
+    const int tile = rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+    const int ra = tile * (2 * kRdLines) + 2 * c;   // real rows ra, ra + 1
     const bool oka = ra < rows, okb = ra + 1 < rows;
     const idx_t ia = (oka ? ra : 0) * N, ib = (okb ? ra + 1 : 0) * N;
     const bool fwd = (kind == K_DCT2 || kind == K_DST2);
