@@ -107,6 +107,7 @@ struct Ctx {
     bool use_fork = true;       // independent per-component passes on forked streams (SMADFT_FORK=0: off)
     bool use_plane = false;
     bool rdz_rev = true;        // z passes walk their tiles from the last row down (SMADFT_RDZ_REV=0: up)
+    bool rdz_static_kind = true;   // z passes specialised per transform kind (SMADFT_RDZ_KIND=0: not)
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -268,8 +269,8 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
 }
 
 // plain z pass of length N through the register-direct z kernel (in == out allowed)
-template <typename T, int N>
-int launch_rdz(Ctx &c, int kind, const T *in, T *out)
+template <typename T, int N, int KIND>
+int launch_rdz_k(Ctx &c, int kind, const T *in, T *out)
 {
     const PlanDev &pd = c.plans.at(N);
     const int rows = c.g.nx * c.g.ny;
@@ -279,16 +280,30 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
     {
         std::lock_guard<std::mutex> lock(attr_mutex());
         if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_rdz_kernel<T, N><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+    r2r_rdz_kernel<T, N, KIND><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h),
         c.rdz_rev ? 1 : 0);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
     return SMADFT_OK;
+}
+
+// plain z pass: one instantiation per transform kind (SMADFT_RDZ_KIND=0: the kind at run time)
+template <typename T, int N>
+int launch_rdz(Ctx &c, int kind, const T *in, T *out)
+{
+    if (!c.rdz_static_kind) return launch_rdz_k<T, N, -1>(c, kind, in, out);
+    switch (kind) {
+    case K_DCT2: return launch_rdz_k<T, N, K_DCT2>(c, kind, in, out);
+    case K_DCT3: return launch_rdz_k<T, N, K_DCT3>(c, kind, in, out);
+    case K_DST2: return launch_rdz_k<T, N, K_DST2>(c, kind, in, out);
+    default: return launch_rdz_k<T, N, K_DST3>(c, kind, in, out);
+    }
 }
 
 // Line lengths with a compile-time staged kernel (the configs' grids); others use the

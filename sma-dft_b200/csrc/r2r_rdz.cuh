@@ -26,11 +26,14 @@ constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * s
 // rev = 1 walks the tiles from the last row down: the pass before a z pass (the y pass of the
 // same transform) writes its field from x = 0 up, so the rows it wrote last, still in L2,
 // are read first.  Tiles are independent, so the order does not change the result.
-template <typename T, int N>
-__global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind, const T *in, T *out,
+// KIND >= 0 fixes the transform kind at compile time (the kind checks inside the transform
+// and the position maps fold away); KIND = -1 takes it from `kind_rt`.
+template <typename T, int N, int KIND = -1>
+__global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind_rt, const T *in, T *out,
                                                                         const cpx<T> *__restrict__ wt_g,
                                                                         const cpx<T> *__restrict__ ht_g, int rev)
 {
+    const int kind = KIND >= 0 ? KIND : kind_rt;
     using RI = RdInfo<N>;
     constexpr int R0 = RI::R0, R1 = RI::R1, NT = RI::THREADS;
     constexpr int BPT = R0 / R1 > 0 ? R0 / R1 : 1;
