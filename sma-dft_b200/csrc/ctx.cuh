@@ -108,6 +108,7 @@ struct Ctx {
     bool use_plane = false;
     bool rdz_rev = true;        // z passes walk their tiles from the last row down (SMADFT_RDZ_REV=0: up)
     bool rdz_static_kind = true;   // z passes specialised per transform kind (SMADFT_RDZ_KIND=0: not)
+    bool rd_static_kind = true;    // plain strided passes specialised per kind (SMADFT_RD_KIND=0: not)
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -210,8 +211,8 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
-template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
-int launch_rd(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
+template <typename T, int N, int AXIS, class LD, class ST, int NC, int KIND>
+int launch_rd_k(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
 {
     const PlanDev &pd = c.plans.at(N);
     const int tiles_b = (c.g.nz + 31) / 32;
@@ -221,16 +222,41 @@ int launch_rd(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
     {
         std::lock_guard<std::mutex> lock(attr_mutex());
         if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC>,
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_rd_kernel<T, N, AXIS, LD, ST, NC><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+    r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         c.g, kinds, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
     return SMADFT_OK;
+}
+
+// strided pass: one-component passes run an instantiation per transform kind
+// (SMADFT_RD_KIND=0: the kind at run time): plain ones (LoadArr -> StoreArr, the bulk of a
+// step) for all four kinds, passes with fused loaders or storers for the cosine kinds they
+// use (their sine passes and the grouped passes take the kind at run time)
+template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
+int launch_rd(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
+{
+    if constexpr (NC == 1) {
+        if (c.rd_static_kind) {
+            constexpr bool plain = std::is_same<LD, LoadArr<T>>::value && std::is_same<ST, StoreArr<T>>::value;
+            switch (kinds.k[0]) {
+            case K_DCT2: return launch_rd_k<T, N, AXIS, LD, ST, 1, K_DCT2>(c, kinds, ld, st);
+            case K_DCT3: return launch_rd_k<T, N, AXIS, LD, ST, 1, K_DCT3>(c, kinds, ld, st);
+            case K_DST2:
+                if constexpr (plain) return launch_rd_k<T, N, AXIS, LD, ST, 1, K_DST2>(c, kinds, ld, st);
+                break;
+            default:
+                if constexpr (plain) return launch_rd_k<T, N, AXIS, LD, ST, 1, K_DST3>(c, kinds, ld, st);
+                break;
+            }
+        }
+    }
+    return launch_rd_k<T, N, AXIS, LD, ST, NC, -1>(c, kinds, ld, st);
 }
 
 // z passes run more CTAs per SM (fewer registers); strided passes keep two

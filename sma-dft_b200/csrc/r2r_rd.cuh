@@ -328,7 +328,9 @@ struct RdPos {
 
 // NC > 1: multi-component pass (LoadMulti / StoreMulti); CTA b transforms component b mod NC
 // of tile b / NC, so the components' shared input reads meet in L2.
-template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
+// KIND >= 0 fixes the transform kind of a one-component pass at compile time (the kind
+// checks inside the transform and the position maps fold away); KIND = -1 reads `kinds`.
+template <typename T, int N, int AXIS, class LD, class ST, int NC = 1, int KIND = -1>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()) r2r_rd_kernel(Geom g, KindSet<NC> kinds, int tiles_b, LD ld,
                                                                        const cpx<T> *__restrict__ wt_g,
                                                                        const cpx<T> *__restrict__ ht_g, ST st)
@@ -355,7 +357,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()
     // tile: 32 k-columns starting at kt*32 along the non-transformed line coordinate `a`
     const int comp = NC > 1 ? (int)(blockIdx.x % NC) : 0;
     const int bt = NC > 1 ? (int)(blockIdx.x / NC) : (int)blockIdx.x;
-    const int kind = kinds.k[comp];
+    const int kind = KIND >= 0 ? KIND : kinds.k[comp];
     const int kt = bt % tiles_b;
     const int a = bt / tiles_b;
     const int k = kt * 32 + 2 * c;                 // first of the two real lines

@@ -432,6 +432,7 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     if (const char *e = std::getenv("SMADFT_FORK")) c.use_fork = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_RDZ_REV")) c.rdz_rev = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_RDZ_KIND")) c.rdz_static_kind = e[0] != '0';
+    if (const char *e = std::getenv("SMADFT_RD_KIND")) c.rd_static_kind = e[0] != '0';
     auto bail = [&](int code) { smadft_destroy(h); return code; };
     if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
