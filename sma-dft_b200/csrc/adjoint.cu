@@ -685,7 +685,7 @@ int adv_adjoint(Ctx &c, const smadft_adj_opts &o, smadft_grads *out, double *dps
                 const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
                 const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
                 T *const o3[3] = {dx, dy, dz};
-                if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, o3, LdNegTG<T, 0>{tA, gx}, LdNegTG<T, 1>{tA, gy},
+                if ((rc = r2r3d_multi<T, 3, 1>(c, kx, ky, kz, o3, LdNegTG<T, 0>{tA, gx}, LdNegTG<T, 1>{tA, gy},
                                             LdNegTG<T, 2>{tA, gz})))
                     return rc;
             }
@@ -694,7 +694,7 @@ int adv_adjoint(Ctx &c, const smadft_adj_opts &o, smadft_grads *out, double *dps
                 const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
                 const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
                 T *const o3[3] = {aSx, aSy, aSz};
-                if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, o3, LdStokesT<T, 0>{sT, dx, dy, dz},
+                if ((rc = r2r3d_multi<T, 3, 0>(c, kx, ky, kz, o3, LdStokesT<T, 0>{sT, dx, dy, dz},
                                             LdStokesT<T, 1>{sT, dx, dy, dz}, LdStokesT<T, 2>{sT, dx, dy, dz})))
                     return rc;
             }
@@ -707,7 +707,7 @@ int adv_adjoint(Ctx &c, const smadft_adj_opts &o, smadft_grads *out, double *dps
                 const int ky[5] = {K_DCT2, K_DCT2, K_DCT2, K_DST2, K_DCT2};
                 const int kz[5] = {K_DCT2, K_DCT2, K_DCT2, K_DCT2, K_DST2};
                 T *const o5[5] = {x1, x2, dx, dy, dz};
-                if ((rc = r2r3d_multi<T, 5>(c, kx, ky, kz, o5,
+                if ((rc = r2r3d_multi<T, 5, 1>(c, kx, ky, kz, o5,
                                             LdAdjPsi<T>{tA, aSx, aSy, aSz, gx, gy, gz, psi, sT.beta, sT.gamma},
                                             LdAdjMu<T>{aSx, aSy, aSz, gx, gy, gz},
                                             LdAdjG<T, 0>{tA, vx, aSx, sp2, psi, sT.beta, sT.gamma},

@@ -279,7 +279,7 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
         const int ky[4] = {K_DCT3, K_DCT3, K_DST3, K_DCT3};
         const int kz[4] = {K_DCT3, K_DCT3, K_DCT3, K_DST3};
         T *const out[4] = {dfd, gx, gy, gz};
-        if ((rc = r2r3d_multi<T, 4>(c, kx, ky, kz, out, LdDfd<T>{s, ph}, LdGrad<T, 0, double>{s, ph},
+        if ((rc = r2r3d_multi<T, 4, 0>(c, kx, ky, kz, out, LdDfd<T>{s, ph}, LdGrad<T, 0, double>{s, ph},
                                     LdGrad<T, 1, double>{s, ph}, LdGrad<T, 2, double>{s, ph})))
             return rc;
     }
@@ -288,7 +288,7 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
         const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
         const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
         T *const out[3] = {rx, ry, rz};
-        if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdGrad<T, 0>{s, rq}, LdGrad<T, 1>{s, rq}, LdGrad<T, 2>{s, rq})))
+        if ((rc = r2r3d_multi<T, 3, 0>(c, kx, ky, kz, out, LdGrad<T, 0>{s, rq}, LdGrad<T, 1>{s, rq}, LdGrad<T, 2>{s, rq})))
             return rc;
     }
     // amplitude: filtered sqrt(q0^2 psi^2 + |grad psi|^2) (:1478-1515), via rq (free now)
@@ -314,7 +314,7 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
         const int kz[8] = {K_DCT2, K_DCT2, K_DCT2, K_DCT2, K_DST2, K_DCT2, K_DCT2, K_DST2};
         T *const out[8] = {fg, en, Sx, Sy, Sz, fx, fy, fz};
         const T e = s.eps, b = s.beta, g = s.gamma, z = s.zeta, kp = s.kp, r0 = s.rho0;
-        if ((rc = r2r3d_multi<T, 8>(
+        if ((rc = r2r3d_multi<T, 8, 1>(
                  c, kx, ky, kz, out, LdCForce<T, 0>{psi, dfd, lap, rho, amp, nullptr, nullptr, mu, e, b, g, z, kp, r0},
                  LdCForce<T, 1>{psi, dfd, lap, rho, amp, nullptr, nullptr, nullptr, e, b, g, z, kp, r0},
                  LdCForce<T, 2>{psi, dfd, lap, rho, amp, gx, rx, nullptr, e, b, g, z, kp, r0},
@@ -345,7 +345,7 @@ int comp_step(Ctx &c, long long nloop, bool keep_old)
         if (plane_ok(c)) {
             for (int m = 0; m < 8; m++)
                 if ((rc = r2r3d<T>(c, kx[m], ky[m], kz[m], LoadArr<T>{out[m]}, StoreArr<T>{out[m]}))) return rc;
-        } else if ((rc = r2r3d_multi<T, 8>(c, kx, ky, kz, out, LoadArr<T>{vsx}, LoadArr<T>{vsy}, LoadArr<T>{vsz},
+        } else if ((rc = r2r3d_multi<T, 8, 0>(c, kx, ky, kz, out, LoadArr<T>{vsx}, LoadArr<T>{vsy}, LoadArr<T>{vsz},
                                            LoadArr<T>{vix}, LoadArr<T>{viy}, LoadArr<T>{viz}, LoadArr<T>{dv},
                                            LoadArr<T>{ad})))
             return rc;

@@ -109,6 +109,7 @@ struct Ctx {
     bool rdz_rev = true;        // z passes walk their tiles from the last row down (SMADFT_RDZ_REV=0: up)
     bool rdz_static_kind = true;   // z passes specialised per transform kind (SMADFT_RDZ_KIND=0: not)
     bool rd_static_kind = true;    // plain strided passes specialised per kind (SMADFT_RD_KIND=0: not)
+    bool rd_static_dir = true;     // grouped passes specialised per direction (SMADFT_RD_DIR=0: not)
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -211,7 +212,7 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
-template <typename T, int N, int AXIS, class LD, class ST, int NC, int KIND>
+template <typename T, int N, int AXIS, class LD, class ST, int NC, int KIND, int DIR = -1>
 int launch_rd_k(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
 {
     const PlanDev &pd = c.plans.at(N);
@@ -222,12 +223,12 @@ int launch_rd_k(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
     {
         std::lock_guard<std::mutex> lock(attr_mutex());
         if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND>,
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND, DIR>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+    r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND, DIR><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         c.g, kinds, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
@@ -238,9 +239,13 @@ int launch_rd_k(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
 // (SMADFT_RD_KIND=0: the kind at run time): plain ones (LoadArr -> StoreArr, the bulk of a
 // step) for all four kinds, passes with fused loaders or storers for the cosine kinds they
 // use (their sine passes and the grouped passes take the kind at run time)
-template <typename T, int N, int AXIS, class LD, class ST, int NC = 1>
+template <typename T, int N, int AXIS, class LD, class ST, int NC = 1, int DIR = -1>
 int launch_rd(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
 {
+    if constexpr (NC > 1 && DIR >= 0) {
+        // grouped pass whose caller states the direction (SMADFT_RD_DIR=0: at run time)
+        if (c.rd_static_dir) return launch_rd_k<T, N, AXIS, LD, ST, NC, -1, DIR>(c, kinds, ld, st);
+    }
     if constexpr (NC == 1) {
         if (c.rd_static_kind) {
             constexpr bool plain = std::is_same<LD, LoadArr<T>>::value && std::is_same<ST, StoreArr<T>>::value;
@@ -516,10 +521,22 @@ int forked(Ctx &c, int n, F fn)
 // to field out[m] with kinds (kx[m], ky[m], kz[m]).  Plane path: one plane launch for all
 // components (their shared reads meet in L2), then the x pass of each in place; otherwise
 // NC separate transforms through the scratch field.
-template <typename T, int NC, class... L>
+template <typename T, int NC, int DIR = -1, class... L>
 int r2r3d_multi(Ctx &c, const int (&kx)[NC], const int (&ky)[NC], const int (&kz)[NC], T *const (&out)[NC], L... ls)
 {
     static_assert(sizeof...(L) == NC, "one loader per component");
+    if constexpr (DIR >= 0) {   // the stated direction must be every component's
+        for (int m = 0; m < NC; m++) {
+            const int want = DIR == 1 ? ((kx[m] == K_DCT2 || kx[m] == K_DST2) && (ky[m] == K_DCT2 || ky[m] == K_DST2) &&
+                                         (kz[m] == K_DCT2 || kz[m] == K_DST2))
+                                      : ((kx[m] == K_DCT3 || kx[m] == K_DST3) && (ky[m] == K_DCT3 || ky[m] == K_DST3) &&
+                                         (kz[m] == K_DCT3 || kz[m] == K_DST3));
+            if (!want) {
+                c.err = "r2r3d_multi: component kinds do not match the stated direction";
+                return SMADFT_ERR_INVALID;
+            }
+        }
+    }
     int rc = SMADFT_OK;
     if (plane_ok(c)) {
         PlaneKinds<NC> pk;
@@ -541,10 +558,12 @@ int r2r3d_multi(Ctx &c, const int (&kx)[NC], const int (&ky)[NC], const int (&kz
             ks.k[m] = ky[m];
             sm.p[m] = out[m];
         }
+        using LM = decltype(make_multi(ls...));
+        using SM = StoreMulti<T, NC>;
         switch (c.g.ny) {
-        case 64: rc = launch_rd<T, 64, 1>(c, ks, make_multi(ls...), sm); break;
-        case 128: rc = launch_rd<T, 128, 1>(c, ks, make_multi(ls...), sm); break;
-        default: rc = launch_rd<T, 256, 1>(c, ks, make_multi(ls...), sm); break;
+        case 64: rc = launch_rd<T, 64, 1, LM, SM, NC, DIR>(c, ks, make_multi(ls...), sm); break;
+        case 128: rc = launch_rd<T, 128, 1, LM, SM, NC, DIR>(c, ks, make_multi(ls...), sm); break;
+        default: rc = launch_rd<T, 256, 1, LM, SM, NC, DIR>(c, ks, make_multi(ls...), sm); break;
         }
         if (rc) return rc;
         return forked(c, NC, [&](int m) {

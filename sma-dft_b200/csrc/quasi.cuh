@@ -306,7 +306,7 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
         const int ky[4] = {K_DCT3, K_DCT3, K_DST3, K_DCT3};
         const int kz[4] = {K_DCT3, K_DCT3, K_DCT3, K_DST3};
         T *const out[4] = {dfd, gx, gy, gz};
-        if ((rc = r2r3d_multi<T, 4>(c, kx, ky, kz, out, LdDfd<T>{s, ph}, LdGrad<T, 0, double>{s, ph},
+        if ((rc = r2r3d_multi<T, 4, 0>(c, kx, ky, kz, out, LdDfd<T>{s, ph}, LdGrad<T, 0, double>{s, ph},
                                     LdGrad<T, 1, double>{s, ph}, LdGrad<T, 2, double>{s, ph})))
             return rc;
     }
@@ -315,7 +315,7 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
         const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
         const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
         T *const out[3] = {rx, ry, rz};
-        if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdGrad<T, 0>{s, rq}, LdGrad<T, 1>{s, rq}, LdGrad<T, 2>{s, rq})))
+        if ((rc = r2r3d_multi<T, 3, 0>(c, kx, ky, kz, out, LdGrad<T, 0>{s, rq}, LdGrad<T, 1>{s, rq}, LdGrad<T, 2>{s, rq})))
             return rc;
     }
     // density law + filter (:1322-1357)
@@ -343,7 +343,7 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
         const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
         const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
         T *const out[3] = {Sx, Sy, Sz};
-        if ((rc = r2r3d_multi<T, 3>(
+        if ((rc = r2r3d_multi<T, 3, 1>(
                  c, kx, ky, kz, out,
                  LdQForce<T, 0>{psi, dfd, lap, rho, gx, rx, mu, en, s.eps, s.beta, s.gamma, lap_rho},
                  LdQForce<T, 1>{psi, dfd, lap, rho, gy, ry, nullptr, nullptr, s.eps, s.beta, s.gamma, lap_rho},
@@ -356,7 +356,7 @@ int quasi_step(Ctx &c, long long nloop, bool keep_old)
         const int ky[4] = {K_DCT3, K_DCT3, K_DST3, K_DCT3};
         const int kz[4] = {K_DCT3, K_DCT3, K_DCT3, K_DST3};
         T *const out[4] = {pp, vx, vy, vz};
-        if ((rc = r2r3d_multi<T, 4>(c, kx, ky, kz, out, LdPressure<T>{s, Sx, Sy, Sz, dv},
+        if ((rc = r2r3d_multi<T, 4, 0>(c, kx, ky, kz, out, LdPressure<T>{s, Sx, Sy, Sz, dv},
                                     LdStokes<T, 0, true>{s, Sx, Sy, Sz, dv}, LdStokes<T, 1, true>{s, Sx, Sy, Sz, dv},
                                     LdStokes<T, 2, true>{s, Sx, Sy, Sz, dv})))
             return rc;

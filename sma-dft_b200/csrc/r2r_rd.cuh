@@ -330,7 +330,9 @@ struct RdPos {
 // of tile b / NC, so the components' shared input reads meet in L2.
 // KIND >= 0 fixes the transform kind of a one-component pass at compile time (the kind
 // checks inside the transform and the position maps fold away); KIND = -1 reads `kinds`.
-template <typename T, int N, int AXIS, class LD, class ST, int NC = 1, int KIND = -1>
+// DIR >= 0 fixes only the direction (1 forward kinds, 0 inverse kinds), which the components
+// of a grouped pass share; the sine/cosine choice then stays per component.
+template <typename T, int N, int AXIS, class LD, class ST, int NC = 1, int KIND = -1, int DIR = -1>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()) r2r_rd_kernel(Geom g, KindSet<NC> kinds, int tiles_b, LD ld,
                                                                        const cpx<T> *__restrict__ wt_g,
                                                                        const cpx<T> *__restrict__ ht_g, ST st)
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()
     const idx_t base = (AXIS == 1 ? a * g.nyz : a * g.nz) + k;
     const int nk = g.nz - k;                       // real lines of this pair inside the box
     const bool full = (kt + 1) * 32 <= g.nz;       // CTA-uniform: no line outside the box
-    const bool fwd = (kind == K_DCT2 || kind == K_DST2);
+    const bool fwd = DIR >= 0 ? DIR == 1 : (kind == K_DCT2 || kind == K_DST2);
     const bool sine = (kind == K_DST2 || kind == K_DST3);
     __syncthreads();
 

@@ -22,7 +22,7 @@ int adv_fields(Ctx &c)
         const int ky[5] = {K_DCT3, K_DCT3, K_DST3, K_DCT3, K_DCT3};
         const int kz[5] = {K_DCT3, K_DCT3, K_DCT3, K_DST3, K_DCT3};
         T *const out[5] = {psi, gx, gy, gz, sp2};
-        if ((rc = r2r3d_multi<T, 5>(c, kx, ky, kz, out, LoadArr<T, double>{ph}, LdGrad<T, 0, double>{s, ph},
+        if ((rc = r2r3d_multi<T, 5, 0>(c, kx, ky, kz, out, LoadArr<T, double>{ph}, LdGrad<T, 0, double>{s, ph},
                                     LdGrad<T, 1, double>{s, ph}, LdGrad<T, 2, double>{s, ph}, LdNegLin<T>{s, ph})))
             return rc;
     }
@@ -32,7 +32,7 @@ int adv_fields(Ctx &c)
         const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
         const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
         T *const out[3] = {Sx, Sy, Sz};
-        if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdForce<T>{psi, sp2, gx, s.beta, s.gamma},
+        if ((rc = r2r3d_multi<T, 3, 1>(c, kx, ky, kz, out, LdForce<T>{psi, sp2, gx, s.beta, s.gamma},
                                     LdForce<T>{psi, sp2, gy, s.beta, s.gamma},
                                     LdForce<T>{psi, sp2, gz, s.beta, s.gamma})))
             return rc;
@@ -43,7 +43,7 @@ int adv_fields(Ctx &c)
         const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
         const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
         T *const out[3] = {vx, vy, vz};
-        if ((rc = r2r3d_multi<T, 3>(c, kx, ky, kz, out, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr},
+        if ((rc = r2r3d_multi<T, 3, 0>(c, kx, ky, kz, out, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr},
                                     LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr},
                                     LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr})))
             return rc;

@@ -156,7 +156,7 @@ int surface_step(Ctx &c, SurfaceScratch &sc)
     {
         const int kk[4] = {K_DCT3, K_DCT3, K_DCT3, K_DCT3};
         T *const out[4] = {f[0], f[1], f[2], f[3]};
-        if ((rc = r2r3d_multi<T, 4>(c, kk, kk, kk, out, LdSurfDt<T>{s, sc.psih_prev, c.f<T>(S_NP), T(c.scale)},
+        if ((rc = r2r3d_multi<T, 4, 0>(c, kk, kk, kk, out, LdSurfDt<T>{s, sc.psih_prev, c.f<T>(S_NP), T(c.scale)},
                                     LdSurfD2<T, 0>{s, sc.psih_prev}, LdSurfD2<T, 1>{s, sc.psih_prev},
                                     LdSurfD2<T, 2>{s, sc.psih_prev})))
             return rc;
