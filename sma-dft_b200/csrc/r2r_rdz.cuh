@@ -28,7 +28,10 @@ constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * s
 // are read first.  Tiles are independent, so the order does not change the result.
 // KIND >= 0 fixes the transform kind at compile time (the kind checks inside the transform
 // and the position maps fold away); KIND = -1 takes it from `kind_rt`.
-template <typename T, int N, int KIND = -1>
+// STAGE: the outputs go through shared memory and leave as whole rows in 16-byte stores (the
+// inverse kinds' Makhoul order would otherwise scatter every warp store over every second
+// element); `out` must then be 16-byte aligned.
+template <typename T, int N, int KIND = -1, bool STAGE = false>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind_rt, const T *in, T *out,
                                                                         const cpx<T> *__restrict__ wt_g,
                                                                         const cpx<T> *__restrict__ ht_g, int rev)
@@ -75,13 +78,37 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     __syncthreads();                                 // twiddle tables
     cpx<T> x1[BPT][R1];
     rd_fft<T, N, true>(v, x1, buf + c * RI::LD, wt, ht, j, threadIdx.x >> 5, fwd, sine, wz);
-    T *qa = out + ia, *qb = out + ib;
+    if constexpr (STAGE) {
+        // the CTA's 2 kRdLines rows in shared memory (inside the exchange buffer), then rows
+        // of N elements out with 16-byte stores; rows past `rows` are not written
+        T *sb = reinterpret_cast<T *>(buf);
+        __syncthreads();                                 // every warp is done with buf
 #pragma unroll
-    for (int pnt = 0; pnt < NP; pnt++) {
-        const cpx<T> z = x1[pnt / R1][pnt % R1];
-        const int o = pos.out(pnt);
-        if (oka) qa[o] = z.x;
-        if (okb) qb[o] = z.y;
+        for (int pnt = 0; pnt < NP; pnt++) {
+            const cpx<T> z = x1[pnt / R1][pnt % R1];
+            const int o = pos.out(pnt);
+            sb[(2 * c) * N + o] = z.x;
+            sb[(2 * c + 1) * N + o] = z.y;
+        }
+        __syncthreads();
+        constexpr int VEC = 16 / (int)sizeof(T);
+        constexpr int PER_ROW = N / VEC;
+        const int row0 = tile * (2 * kRdLines);
+        for (int e = threadIdx.x; e < 2 * kRdLines * PER_ROW; e += NT) {
+            const int r = e / PER_ROW, cv = e % PER_ROW;
+            if (row0 + r < rows)
+                *reinterpret_cast<uint4 *>(out + (idx_t)(row0 + r) * N + cv * VEC) =
+                    *reinterpret_cast<const uint4 *>(sb + r * N + cv * VEC);
+        }
+    } else {
+        T *qa = out + ia, *qb = out + ib;
+#pragma unroll
+        for (int pnt = 0; pnt < NP; pnt++) {
+            const cpx<T> z = x1[pnt / R1][pnt % R1];
+            const int o = pos.out(pnt);
+            if (oka) qa[o] = z.x;
+            if (okb) qb[o] = z.y;
+        }
     }
 }
 
