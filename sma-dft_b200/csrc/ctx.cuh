@@ -112,7 +112,6 @@ struct Ctx {
     bool rd_static_kind = true;    // plain strided passes specialised per kind (SMADFT_RD_KIND=0: not)
     bool rd_static_dir = true;     // grouped passes specialised per direction (SMADFT_RD_DIR=0: not)
     bool rdz_stage = true;         // inverse z passes stage their outputs in shared memory (SMADFT_RDZ_STAGE=0: not)
-    bool rdz_stage_in = false;     // z passes stage their inputs in shared memory (SMADFT_RDZ_STAGE_IN=1: do)
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -303,7 +302,7 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
 }
 
 // plain z pass of length N through the register-direct z kernel (in == out allowed)
-template <typename T, int N, int KIND, int STG = 0>
+template <typename T, int N, int KIND, bool STAGE = false>
 int launch_rdz_k(Ctx &c, int kind, const T *in, T *out)
 {
     const PlanDev &pd = c.plans.at(N);
@@ -314,12 +313,12 @@ int launch_rdz_k(Ctx &c, int kind, const T *in, T *out)
     {
         std::lock_guard<std::mutex> lock(attr_mutex());
         if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N, KIND, STG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N, KIND, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem));
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_rdz_kernel<T, N, KIND, STG><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+    r2r_rdz_kernel<T, N, KIND, STAGE><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h),
         c.rdz_rev ? 1 : 0);
     SMADFT_CUDA(cudaGetLastError());
@@ -332,27 +331,15 @@ template <typename T, int N>
 int launch_rdz(Ctx &c, int kind, const T *in, T *out)
 {
     if (!c.rdz_static_kind) return launch_rdz_k<T, N, -1>(c, kind, in, out);
-    // inverse kinds stage their outputs through shared memory when `out` allows 16-byte stores;
-    // every kind stages its inputs when `in` allows 16-byte loads (and rdz_stage_in is set)
-    const int so = (c.rdz_stage && ((uintptr_t)out & 15) == 0) ? 1 : 0;
-    const int si = (c.rdz_stage_in && ((uintptr_t)in & 15) == 0) ? 2 : 0;
+    // inverse kinds stage their outputs through shared memory when `out` allows 16-byte stores
+    const bool stage = c.rdz_stage && ((uintptr_t)out & 15) == 0;
     switch (kind) {
-    case K_DCT2: return si ? launch_rdz_k<T, N, K_DCT2, 2>(c, kind, in, out) : launch_rdz_k<T, N, K_DCT2>(c, kind, in, out);
-    case K_DST2: return si ? launch_rdz_k<T, N, K_DST2, 2>(c, kind, in, out) : launch_rdz_k<T, N, K_DST2>(c, kind, in, out);
+    case K_DCT2: return launch_rdz_k<T, N, K_DCT2>(c, kind, in, out);
     case K_DCT3:
-        switch (so | si) {
-        case 3: return launch_rdz_k<T, N, K_DCT3, 3>(c, kind, in, out);
-        case 2: return launch_rdz_k<T, N, K_DCT3, 2>(c, kind, in, out);
-        case 1: return launch_rdz_k<T, N, K_DCT3, 1>(c, kind, in, out);
-        default: return launch_rdz_k<T, N, K_DCT3>(c, kind, in, out);
-        }
+        return stage ? launch_rdz_k<T, N, K_DCT3, true>(c, kind, in, out) : launch_rdz_k<T, N, K_DCT3>(c, kind, in, out);
+    case K_DST2: return launch_rdz_k<T, N, K_DST2>(c, kind, in, out);
     default:
-        switch (so | si) {
-        case 3: return launch_rdz_k<T, N, K_DST3, 3>(c, kind, in, out);
-        case 2: return launch_rdz_k<T, N, K_DST3, 2>(c, kind, in, out);
-        case 1: return launch_rdz_k<T, N, K_DST3, 1>(c, kind, in, out);
-        default: return launch_rdz_k<T, N, K_DST3>(c, kind, in, out);
-        }
+        return stage ? launch_rdz_k<T, N, K_DST3, true>(c, kind, in, out) : launch_rdz_k<T, N, K_DST3>(c, kind, in, out);
     }
 }
 

@@ -4,16 +4,15 @@
 // The strided kernel puts 16 lines on the lanes of a half-warp so that one access covers
 // 128 contiguous bytes.  Along z a line is itself contiguous, so here the R1 lanes of a
 // line group are the first-stage butterflies j of one packed complex line (real rows
-// r and r + 1 as real and imaginary parts).  Butterfly j takes the positions of its
-// points j + R1 q: consecutive lanes read consecutive positions (inverse kinds) or every
-// second one (the Makhoul order of the forward kinds, whose other half the same warp
-// reads in another instruction).  Unstaged, these are scalar loads straight from global
-// memory (every 32-byte sector a warp touches is used in full); staged (STG bit 2), the
-// CTA's rows first come into shared memory as 16-byte loads, a quarter (FP32) or half
-// (FP64) of the load instructions.  The exchange between the two radix stages goes
-// through shared memory; the X[p] / X[N - p] pairings are lane shuffles inside the line
-// group (rd_fft, ZMAP).  Loads finish before the first barrier after them and every row
-// belongs to one CTA, so the pass may run in place (in == out).
+// r and r + 1 as real and imaginary parts).  Butterfly j reads the positions of its
+// points j + R1 q straight from global memory into registers: consecutive lanes read
+// consecutive positions (inverse kinds) or every second one (the Makhoul order of the
+// forward kinds, whose other half the same warp reads in another instruction), so each
+// 32-byte sector a warp touches is used in full and the tile is never staged in shared
+// memory.  Shared memory carries only the exchange between the two radix stages; the
+// X[p] / X[N - p] pairings are lane shuffles inside the line group (rd_fft, ZMAP).
+// Outputs go from registers to global memory.  Loads finish before the first barrier and
+// every row belongs to one CTA, so the pass may run in place (in == out).
 #pragma once
 
 #include "r2r_rd.cuh"
@@ -29,12 +28,10 @@ constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * s
 // are read first.  Tiles are independent, so the order does not change the result.
 // KIND >= 0 fixes the transform kind at compile time (the kind checks inside the transform
 // and the position maps fold away); KIND = -1 takes it from `kind_rt`.
-// STG bit 1: the outputs go through shared memory and leave as whole rows in 16-byte stores
-// (the inverse kinds' Makhoul order would otherwise scatter every warp store over every
-// second element); `out` must then be 16-byte aligned.  STG bit 2: the inputs come in the
-// same way, whole rows in 16-byte loads, and each thread picks its points from shared
-// memory; `in` must then be 16-byte aligned.
-template <typename T, int N, int KIND = -1, int STG = 0>
+// STAGE: the outputs go through shared memory and leave as whole rows in 16-byte stores (the
+// inverse kinds' Makhoul order would otherwise scatter every warp store over every second
+// element); `out` must then be 16-byte aligned.
+template <typename T, int N, int KIND = -1, bool STAGE = false>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind_rt, const T *in, T *out,
                                                                         const cpx<T> *__restrict__ wt_g,
                                                                         const cpx<T> *__restrict__ ht_g, int rev)
@@ -64,50 +61,24 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     const bool sine = (kind == K_DST2 || kind == K_DST3);
 
     const RdPos<N> pos(j, fwd, sine);               // affine position maps (r2r_rd.cuh)
-    constexpr int VEC = 16 / (int)sizeof(T);
-    constexpr int PER_ROW = N / VEC;
-    const int row0 = tile * (2 * kRdLines);
+    const T *pa = in + ia, *pb = in + ib;
     cpx<T> v[R0];
-    if constexpr ((STG & 2) != 0) {
-        // the CTA's rows into the exchange buffer (rows past `rows` read as zero)
-        T *sb = reinterpret_cast<T *>(buf);
-        for (int e = threadIdx.x; e < 2 * kRdLines * PER_ROW; e += NT) {
-            const int r = e / PER_ROW, cv = e % PER_ROW;
-            uint4 w = make_uint4(0u, 0u, 0u, 0u);
-            if (row0 + r < rows) w = *reinterpret_cast<const uint4 *>(in + (idx_t)(row0 + r) * N + cv * VEC);
-            *reinterpret_cast<uint4 *>(sb + r * N + cv * VEC) = w;
-        }
-        __syncthreads();                             // staged rows and twiddle tables
 #pragma unroll
-        for (int q = 0; q < R0; q++) {
-            const int n = pos.src(q);
-            T a = sb[(2 * c) * N + n], b = sb[(2 * c + 1) * N + n];
-            if (fwd && sine && !RdPos<N>::src_lo(q)) {   // DST-II negates odd natural samples
-                a = -a;
-                b = -b;
-            }
-            v[q] = {a, b};
+    for (int q = 0; q < R0; q++) {
+        const int n = pos.src(q);
+        T a = pa[n], b = pb[n];
+        if (!oka) a = T(0);
+        if (!okb) b = T(0);
+        if (fwd && sine && !RdPos<N>::src_lo(q)) {   // DST-II negates odd natural samples
+            a = -a;
+            b = -b;
         }
-        __syncthreads();                             // the transform reuses the buffer
-    } else {
-        const T *pa = in + ia, *pb = in + ib;
-#pragma unroll
-        for (int q = 0; q < R0; q++) {
-            const int n = pos.src(q);
-            T a = pa[n], b = pb[n];
-            if (!oka) a = T(0);
-            if (!okb) b = T(0);
-            if (fwd && sine && !RdPos<N>::src_lo(q)) {   // DST-II negates odd natural samples
-                a = -a;
-                b = -b;
-            }
-            v[q] = {a, b};
-        }
-        __syncthreads();                             // twiddle tables
+        v[q] = {a, b};
     }
+    __syncthreads();                                 // twiddle tables
     cpx<T> x1[BPT][R1];
     rd_fft<T, N, true>(v, x1, buf + c * RI::LD, wt, ht, j, threadIdx.x >> 5, fwd, sine, wz);
-    if constexpr ((STG & 1) != 0) {
+    if constexpr (STAGE) {
         // the CTA's 2 kRdLines rows in shared memory (inside the exchange buffer), then rows
         // of N elements out with 16-byte stores; rows past `rows` are not written
         T *sb = reinterpret_cast<T *>(buf);
@@ -120,6 +91,9 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
             sb[(2 * c + 1) * N + o] = z.y;
         }
         __syncthreads();
+        constexpr int VEC = 16 / (int)sizeof(T);
+        constexpr int PER_ROW = N / VEC;
+        const int row0 = tile * (2 * kRdLines);
         for (int e = threadIdx.x; e < 2 * kRdLines * PER_ROW; e += NT) {
             const int r = e / PER_ROW, cv = e % PER_ROW;
             if (row0 + r < rows)

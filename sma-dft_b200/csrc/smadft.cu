@@ -435,7 +435,6 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     if (const char *e = std::getenv("SMADFT_RD_KIND")) c.rd_static_kind = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_RD_DIR")) c.rd_static_dir = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_RDZ_STAGE")) c.rdz_stage = e[0] != '0';
-    if (const char *e = std::getenv("SMADFT_RDZ_STAGE_IN")) c.rdz_stage_in = e[0] != '0';
     auto bail = [&](int code) { smadft_destroy(h); return code; };
     if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
