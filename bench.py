@@ -2,17 +2,20 @@
 """bench.py -- steps/s of sma-dft's advected (adv) time step at 256^3 on B200.
 
 Metric (the reference's headline path): steps/s at 256^3 adv, mixed precision (FP32 fields,
-FP64 reductions) against the plain FP64 GPU step, with the relative L2 error of psi against
-FP64 stated.  Workload: adv/cosAdvTrackMult.cpp-style step, 256x256x256, dx = lambda0/8,
-dt = 0.02, nu = 1, eps = -0.75, alpha = 1, beta = 2, gamma = 1; synthetic seeded IC
-(smectic layers with 4 focal-conic-like perturbations, smadft_ic_conics).
+FP64 spectral state, update and reductions) against the plain FP64 GPU step, with the
+relative L2 error of psi against FP64 stated.  Workload: adv/cosAdvTrackMult.cpp-style step,
+256x256x256, dx = lambda0/8, dt = 0.01, nu = 1, eps = -0.75, alpha = 1, beta = 2, gamma = 1;
+synthetic seeded IC (smectic layers with 4 focal-conic-like perturbations, built in numpy by
+make_ic).  dt = 0.01 rather than the configuration's 0.02: at dx = lambda0/8 the scheme
+diverges at 0.02 (the reference build does too); the cost of a step does not depend on dt.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One process per GPU (torchrun for N > 1).  The path does not shard (one simulation per GPU,
 "replicas only"): every rank runs its own replica, value = all ranks' steps / max time.
 ``--impl reference`` times the reference's own loop body (oracle/_ref/adv_ref: the
-reference sources compiled with single-rank MPI / FFTW-r2r shims) on the host cores.
+reference sources compiled with single-rank MPI / FFTW-r2r shims) on the host cores, for the
+same K steps after W untimed ones; it never loads the product library.
 """
 from __future__ import annotations
 
@@ -21,7 +24,6 @@ import json
 import os
 import re
 import statistics
-import subprocess
 import sys
 import tempfile
 import threading
@@ -41,6 +43,11 @@ N = 256
 CFG = dict(nw=8.0, dt=0.01, eps=-0.75, nu=1.0, alpha=1.0, beta=2.0, gamma=1.0)
 ERR_STEPS = 10000   # steps after which the FP32 psi is compared with the FP64 psi
 F_ADV = 32          # compulsory full-field transfers per adv step (single-sweep stages)
+# the kernel the roofline object describes, its key in pass_kernels and its ncu summary
+DOMINANT_PASS = "z_dct3"
+DOMINANT_PROFILE = "r2r_rdz_z_pass_256cube_fp32.md"
+DOMINANT_KERNEL = ("r2r_rdz_kernel<float,256,DCT-III> plain inverse pass along z (the largest share of the adv "
+                   "step's device time); algorithmic bytes per launch = 2 x 4 B x 256^3, 6-field ring")
 
 
 def peaks():
@@ -53,77 +60,91 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 50 ms.
+    """SM clocks and clock-event (throttle) reasons of one GPU, polled through NVML every
+    2 ms on a host thread (reads only; no setting of the GPU is touched).
 
-    ``start()`` waits (up to 10 s) until the first sample has arrived, so that the sampler is
-    running before the timed region begins; ``mark(t0, t1)`` keeps the samples that arrived
-    inside the timed region (host wall clock).
+    ``mark(t0, t1)`` keeps the samples taken inside the timed region (host wall clock); a
+    timed region of a few tens of milliseconds still holds a dozen samples.  The GPU is found
+    by the UUID torch reports for the CUDA device, so it is the right one under
+    CUDA_VISIBLE_DEVICES.
     """
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_S = 0.002
+    NAMES = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+             ("sw_power_cap", 0x4))
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.lines: list[tuple[float, str]] = []
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
+        self.samples: list[tuple[float, int, int]] = []
         self.window = (0.0, float("inf"))
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
-            t0 = time.time()
-            while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
-                time.sleep(0.02)
-        except Exception:
-            self.proc = None
-        return self
+            h = self._handle()
+            nv = self._nvml
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append((time.time(), line.strip()))
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.time(), int(mhz), int(rs)))
+                    except Exception:
+                        pass
+                    time.sleep(self.INTERVAL_S)
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0:
+                time.sleep(0.001)
+        except Exception:
+            self._thread = None
+        return self
 
     def mark(self, t0: float, t1: float):
         self.window = (t0, t1)
 
     def __exit__(self, *a):
-        if self.proc:
-            time.sleep(0.1)
-            self.proc.terminate()
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=2.0)
+        if self._nvml is not None:
             try:
-                self.proc.wait(timeout=5)
+                self._nvml.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         lo, hi = self.window
-        for ts, ln in self.lines:
-            if not (lo <= ts <= hi):
-                continue
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm), "interval_ms": 50}
+        inside = [(mhz, rs) for ts, mhz, rs in self.samples if lo <= ts <= hi]
+        reasons = sorted({nm for _, rs in inside for nm, bit in self.NAMES if rs & bit})
+        return {"sm_mhz": statistics.median([m for m, _ in inside]) if inside else None,
+                "sm_max_mhz": self.max_mhz, "reasons": reasons, "samples": len(inside),
+                "interval_ms": 1000 * self.INTERVAL_S, "source": "NVML"}
 
 
-def cpu_reference_run(steps: int, psi0: np.ndarray | None, threads: int):
-    """Run the shimmed reference adv loop at 256^3; returns (steps/s, seconds, kind, sample)."""
+def cpu_reference_run(steps: int, psi0: np.ndarray, threads: int):
+    """Run the shimmed reference adv loop at 256^3; returns (steps/s, seconds, kind, sample).
+
+    The reference's own sources (adv/cosAdvTrackMult.cpp) compiled with the single-rank MPI /
+    FFTW-r2r shim (oracle/_ref/adv_ref), timed by the reference's own wall clock around its
+    loop; where that build is absent, the FP64 oracle port of the same loop."""
     import oracle
     shape = (N, N, N)
     if oracle.reference_available("adv"):
@@ -137,34 +158,89 @@ def cpu_reference_run(steps: int, psi0: np.ndarray | None, threads: int):
         secs = float(m.group(1)) if m else wall
         return steps / secs, secs, "reference", (
             f"{steps} steps of the reference adv loop body at 256^3 (adv/cosAdvTrackMult.cpp, "
-            f"single-rank shim, FFTW replaced by the oracle FP64 r2r), timed by its own wall clock")
+            f"single-rank shim, FFTW replaced by the oracle FP64 r2r, {threads} OpenMP threads), "
+            f"timed by its own wall clock")
     o = oracle.Oracle(oracle.ADV, shape, **{k: v for k, v in CFG.items()})
     o.set_psi(psi0)
     t0 = time.perf_counter()
     o.step(steps)
     secs = time.perf_counter() - t0
-    return steps / secs, secs, "port", f"{steps} steps of the FP64 oracle adv step at 256^3"
+    return steps / secs, secs, "port", f"{steps} steps of the FP64 oracle adv step at 256^3, {threads} threads"
 
 
-def make_ic():
-    import smadft
-    p = smadft.params(smadft.ADV, (N, N, N), **CFG)
-    return smadft.ic_conics(p, A=1.328, count=4, rmin=3.0, rmax=6.0, noise=1e-3, seed=20240601)
+def _mix64(z):
+    """SplitMix64 finaliser (Steele, Lea, Flood 2014) on uint64 arrays (wrapping arithmetic)."""
+    z = z + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def _uniform(seed: int, ctr):
+    """Uniform in [0, 1) from (seed, counter): the counter-based stream of the product's IC
+    builders (csrc/ic.cpp), so host and library make identical noise."""
+    x = _mix64(np.uint64(seed) ^ _mix64(np.asarray(ctr, dtype=np.uint64)))
+    return (x >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def make_ic(shape=(N, N, N), A=1.328, count=4, rmin=3.0, rmax=6.0, noise=1e-3, seed=20240601):
+    """Config 3's synthetic initial condition, built on the host in numpy: smectic layers
+    A cos(q0 z) over the smectic half x < L/2 (tanh envelope of width 2 lambda0) with `count`
+    radial focal perturbations (radius rmin..rmax lambda0, centres uniform in the smectic
+    half, blended over one wavelength), plus seeded uniform noise.  The same construction as
+    smadft_ic_conics (node positions x_i = i dx, as adv/cosAdvTrackMult.cpp:500-536 writes its
+    layers); both arms of the benchmark use this array, so the reference arm never loads the
+    product library."""
+    nw, q0 = CFG["nw"], 1.0
+    nx, ny, nz = shape
+    dx = 2.0 * np.pi / (q0 * nw)
+    Lx, Ly, Lz = nx * dx, ny * dx, nz * dx
+    lam0 = 2.0 * np.pi / q0
+    base = 0x5A5A0000 + 16 * np.arange(count, dtype=np.uint64)
+    cx = _uniform(seed, base + np.uint64(0)) * 0.5 * Lx
+    cy = _uniform(seed, base + np.uint64(1)) * Ly
+    cz = _uniform(seed, base + np.uint64(2)) * Lz
+    R = (rmin + (rmax - rmin) * _uniform(seed, base + np.uint64(3))) * lam0
+    x = (np.arange(nx) * dx)[:, None, None]
+    y = (np.arange(ny) * dx)[None, :, None]
+    z = (np.arange(nz) * dx)[None, None, :]
+    layer = np.cos(q0 * z) * np.ones((nx, ny, 1))
+    for c in range(count):
+        d = np.sqrt((x - cx[c]) * (x - cx[c]) + (y - cy[c]) * (y - cy[c]) + (z - cz[c]) * (z - cz[c]))
+        w = 0.5 * (1.0 - np.tanh((d - R[c]) / lam0))
+        layer = w * np.cos(q0 * d) + (1.0 - w) * layer
+    env = 0.5 * (1.0 - np.tanh((x - 0.5 * Lx) / (2.0 * lam0)))
+    psi = A * layer * env
+    if noise != 0.0:
+        psi = psi + noise * (2.0 * _uniform(seed, np.arange(nx * ny * nz, dtype=np.uint64)).reshape(shape) - 1.0)
+    return np.ascontiguousarray(psi)
+
+
+def bench_config(world: int) -> dict:
+    """The workload both arms run (identical in both JSON lines)."""
+    return {"workload": "adv 256^3 time step (cosAdvTrackMult-style)",
+            "grid": [N, N, N], "dt": CFG["dt"], "dx": "lambda0/8", "nu": CFG["nu"], "eps": CFG["eps"],
+            "ic": "smectic layers + 4 seeded focal perturbations (radius 3-6 lambda0), noise 1e-3, seed 20240601",
+            "parallelism": f"replicas x{world}",
+            "l2_flush": "inputs larger than L2 (about 1 GB of fields touched per step)"}
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own loop body on the host cores: W untimed steps in one process, then
+    the K timed steps in a second one (the reference times its loop with its own wall clock),
+    all host threads.  Rank 0 alone runs and prints; other ranks exit without work."""
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    steps = max(1, min(args.steps, 3))
     psi0 = make_ic()
-    sps, secs, kind, sample = cpu_reference_run(steps, psi0, threads)
+    if args.warmup > 0:
+        cpu_reference_run(args.warmup, psi0, threads)
+    sps, secs, kind, sample = cpu_reference_run(args.steps, psi0, threads)
     line = {
         "metric": METRIC, "value": sps, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
-        "steps": steps, "warmup": 0, "ms_per_step": 1000.0 * secs / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "adv 256^3 time step (cosAdvTrackMult-style), dt=0.01, dx=lambda0/8, nu=1",
-                   "grid": [N, N, N], "host_threads": threads},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": bench_config(world),
         "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -228,12 +304,13 @@ def profile_traffic(name: str):
 
 
 def pass_roofline(torch, smadft, peak):
-    """Average launch time of the plain DCT-II pass along each axis of a 256^3 FP32 field.
+    """Average launch time of the plain axis passes of a 256^3 FP32 field, forward (DCT-II)
+    and inverse (DCT-III) kinds along each axis.
 
     The passes run through a ring of 6 fields (384 MiB, well above the 126 MB L2): launch r
     reads field r mod 6 and writes field r+1 mod 6, so every launch reads a field that was
     last written five launches earlier.  Algorithmic bytes per launch = one field read + one
-    field written = 2 x 4 B x 256^3.
+    field written = 2 x 4 B x 256^3.  Times are CUDA events on the context's stream.
     """
     ring = 6
     p = smadft.params(smadft.ADV, (N, N, N), precision=smadft.FP32, **CFG)
@@ -243,23 +320,24 @@ def pass_roofline(torch, smadft, peak):
         stream = torch.cuda.ExternalStream(s.stream)
         out = {}
         for axis, name in ((2, "z"), (1, "y"), (0, "x")):
-            for r in range(ring):
-                s.r2r_pass_device(bufs[r].data_ptr(), bufs[(r + 1) % ring].data_ptr(), axis, 0)
-            reps = 10 * ring
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            ev0.record(stream)
-            for r in range(reps):
-                s.r2r_pass_device(bufs[r % ring].data_ptr(), bufs[(r + 1) % ring].data_ptr(), axis, 0)
-            ev1.record(stream)
-            torch.cuda.synchronize()
-            us = 1000.0 * ev0.elapsed_time(ev1) / reps
-            gbs = 2.0 * 4 * N ** 3 / (us * 1e-6) / 1e9
-            out[name] = {"us": us, "gbs": gbs, "frac": gbs / peak}
-            # refill: repeated unnormalised DCT-II passes grow the values by about 2N each
-            for bft in bufs:
-                bft.normal_()
-            torch.cuda.synchronize()
+            for kind, kname in ((0, "dct2"), (1, "dct3")):
+                for r in range(ring):
+                    s.r2r_pass_device(bufs[r].data_ptr(), bufs[(r + 1) % ring].data_ptr(), axis, kind)
+                reps = 10 * ring
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                ev0.record(stream)
+                for r in range(reps):
+                    s.r2r_pass_device(bufs[r % ring].data_ptr(), bufs[(r + 1) % ring].data_ptr(), axis, kind)
+                ev1.record(stream)
+                torch.cuda.synchronize()
+                us = 1000.0 * ev0.elapsed_time(ev1) / reps
+                gbs = 2.0 * 4 * N ** 3 / (us * 1e-6) / 1e9
+                out[f"{name}_{kname}"] = {"us": round(us, 2), "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+                # refill: repeated unnormalised passes grow the values by about 2N each
+                for bft in bufs:
+                    bft.normal_()
+                torch.cuda.synchronize()
         return out
 
 
@@ -487,43 +565,42 @@ def run_ours(args, rank, world, local_rank):
     achieved_step = algo_bytes / (ms_step * 1e-3) / 1e9
     cpu = {}
     try:
-        sps, secs, kind, sample = cpu_reference_run(4, psi0, os.cpu_count() or 1)
-        cpu = {"value": sps, "unit": "steps/s", "cores": os.cpu_count() or 1, "kind": kind, "sample": sample}
+        threads = os.cpu_count() or 1
+        sps, secs, kind, sample = cpu_reference_run(4, psi0, threads)
+        cpu = {"value": sps, "unit": "steps/s", "cores": threads, "kind": kind, "sample": sample}
     except Exception as e:  # reported, not fatal
         cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
-    zp = passes.get("z", {})
+    # the dominant kernel of the step (largest share of its device time in the committed
+    # launch list): the plain inverse (DCT-III) pass along z
+    dom = passes.get(DOMINANT_PASS, {})
+    config = bench_config(world)
+    config.update({
+        "fp32_ms_per_step": round(ms_step, 4), "fp64_ms_per_step": round(ms_step64, 4),
+        "speedup_vs_fp64": round(ms_step64 / ms_step, 3), "rel_l2_err_vs_fp64": err, "err_after_steps": err_steps,
+        "precision": "FP32 fields and transforms; FP64 spectral state, time update and reductions",
+        "kernel_path": tuned.get("fp32")})
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "adv 256^3 time step (cosAdvTrackMult-style), dt=0.01, dx=lambda0/8, nu=1, "
-                               "eps=-0.75; FP32 fields and transforms, FP64 spectral state, update and reductions",
-                   "grid": [N, N, N], "parallelism": f"replicas x{world}",
-                   "l2_flush": "inputs larger than L2 (about 1 GB of fields touched per step)"},
-        "fp64_steps_per_s": world * args.steps / (res["fp64"]["ms"] / 1000.0),
-        "fp64_ms_per_step": ms_step64,
-        "speedup_vs_fp64": ms_step64 / ms_step,
-        "rel_l2_err_vs_fp64": err,
-        "err_after_steps": err_steps,
-        "rel_l2_err_after_timed_steps": err_timed,
-        "state_precision": "psihat (the spectral state) in FP64, time update in FP64",
-        "autotuned_path": tuned,
-        "roofline": {"bound": "hbm", "achieved": zp.get("gbs"), "peak": peak, "unit": "GB/s",
-                     "frac": zp.get("frac"), "traffic": profile_traffic("r2r_rdz_z_pass_256cube_fp32.md"),
+        "config": config,
+        "roofline": {"bound": "hbm", "achieved": dom.get("gbs"), "peak": peak, "unit": "GB/s",
+                     "frac": dom.get("frac"), "traffic": profile_traffic(DOMINANT_PROFILE),
                      "peak_source": f"{peak_kind} hbm_gbs",
-                     "kernel": "r2r_rdz_kernel<float,256> plain DCT-II pass along z (the largest share of "
-                               "the adv step's device time): algorithmic bytes per launch = 2 x 4 B x 256^3 "
-                               "(one field read, one written), average launch time on a 6-field ring"},
-        "step_roofline": {"achieved": achieved_step, "peak": peak, "unit": "GB/s", "frac": achieved_step / peak,
-                          "basis": "4 B x 256^3 x 32 compulsory field transfers per adv step"},
-        "pass_kernels": passes,
+                     "kernel": DOMINANT_KERNEL,
+                     "step_frac": round(achieved_step / peak, 4)},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 8 * N ** 3,
                 "d2h_bytes_per_step": 8 * N ** 3},
         "gpu_launches": launches_fp32,
+        "clocks": clocks,
+        "fp64_steps_per_s": world * args.steps / (res["fp64"]["ms"] / 1000.0),
+        "rel_l2_err_after_timed_steps": err_timed,
+        "step_roofline": {"achieved": achieved_step, "peak": peak, "unit": "GB/s", "frac": achieved_step / peak,
+                          "basis": "4 B x 256^3 x 32 compulsory field transfers per adv step"},
+        "pass_kernels": passes,
         "batch_sweep": sweep,
         "adjoint": adjoint,
-        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -210,18 +210,22 @@ int smadft_r2r3d_device(smadft_ctx *ctx, const void *in, void *out, int kx, int 
 
 /* The same 3-D r2r transform for callers that cannot allocate device memory.  No
  * counterpart in the reference: FFTW plans own their buffers there.  Some callers cannot
- * call cudaMalloc -- code in a stream callback or cudaLaunchHostFunc host function, code
- * whose device memory is fully reserved by another allocator, or fixed-latency loops where
- * cudaMalloc's implicit device synchronisation is not acceptable.  This entry point needs
- * no context and allocates nothing: the intermediate field lives in a fixed file-scope
- * device array of SMADFT_NOALLOC_MAX_BYTES that every GPU loading the library holds until
- * exit.  Limits: nx*ny*nz*element_size <= SMADFT_NOALLOC_MAX_BYTES (else
- * SMADFT_ERR_TOO_LARGE), lengths even, <= 512, factors 2, 3, 5.  in/out 16-byte aligned
- * device buffers (double* for SMADFT_FP64, float* for SMADFT_FP32); in may equal out.  The
- * work is queued on `stream` (a cudaStream_t, NULL = legacy default stream).  All calls
- * share the array, so calls that overlap on the GPU race; a call needs nothing from earlier
- * calls (it writes every scratch element before reading it).  The first call on a device
- * looks the array up for that device and should come before any stream capture. */
+ * call cudaMalloc: code whose device memory is fully reserved up front by another allocator
+ * (a caching pool, an MPI+CUDA code that carved HBM at start-up), where cudaMalloc fails, and
+ * fixed-latency loops where cudaMalloc's implicit device synchronisation is not acceptable.
+ * This entry point needs no context and allocates nothing: the intermediate field lives in
+ * a fixed file-scope device array of SMADFT_NOALLOC_MAX_BYTES that every GPU loading the
+ * library holds until exit, and the twiddle tables in another (48 KiB), filled by a small
+ * kernel on `stream` (no host copies).  It is an ordinary CUDA host call (it queries the
+ * device and launches kernels): not for stream callbacks or cudaLaunchHostFunc functions,
+ * where CUDA calls are not allowed.  Limits: nx*ny*nz*element_size <=
+ * SMADFT_NOALLOC_MAX_BYTES (else SMADFT_ERR_TOO_LARGE), lengths even, <= 512, factors 2, 3, 5
+ * (else SMADFT_ERR_UNSUPPORTED).  in/out 16-byte aligned device buffers (double* for
+ * SMADFT_FP64, float* for SMADFT_FP32); in may equal out.  The work is queued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream).  All calls share the scratch array and the
+ * twiddle tables, so calls that overlap on the GPU race; a call needs nothing from earlier
+ * calls (it writes every element it reads).  The first call on a device looks the arrays up
+ * for that device and sets kernel attributes; it should come before any stream capture. */
 #define SMADFT_NOALLOC_MAX_BYTES (16u << 20)
 int smadft_r2r3d_noalloc(const void *in, void *out, int nx, int ny, int nz, int kx, int ky, int kz,
                          int precision, void *stream);

@@ -2,7 +2,8 @@
 # build_ref.sh -- compile the reference's own time-step sources into oracle/_ref/ (test
 # infrastructure: the binaries pin the oracle and give the CPU baseline).
 #
-# The sources are read where they lie (SMADFT_REFERENCE, default /root/reference) and are
+# The sources are read where they lie (SMADFT_REFERENCE, default: a "reference" directory
+# beside this repository) and are
 # never copied into the repository: each one is streamed through sed into g++ on stdin.
 # FFTW and MPI are not installed, so the build links the single-rank shim in refshim/.
 # The sed edits only turn hard-coded constants into run-time parameters and add hooks:
@@ -15,8 +16,8 @@
 #   * before MPI::Finalize(), binary dumps of the final fields
 # Usage: oracle/build_ref.sh   (writes oracle/_ref/{noadv,bump,adv,quasi,noadvc,advc,comp}_ref)
 set -euo pipefail
-REF="${SMADFT_REFERENCE:-/root/reference}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
+REF="${SMADFT_REFERENCE:-$HERE/../../reference}"
 OUT="$HERE/_ref"
 CXX="${SMADFT_CXX:-g++}"
 CC="${SMADFT_CC:-gcc}"

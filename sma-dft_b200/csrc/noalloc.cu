@@ -1,26 +1,29 @@
 // noalloc.cu -- smadft_r2r3d_noalloc: the 3-D r2r transform of smadft_r2r3d_device for
 // callers that cannot allocate device memory.
 //
-// Who needs it: code that runs where cudaMalloc is not an option -- inside a stream
-// callback or host function enqueued with cudaLaunchHostFunc (CUDA calls are not allowed
-// there), in applications whose device memory is fully reserved up front by another
-// allocator (a framework's caching pool, an MPI+CUDA code that carved HBM at start-up), or
-// in fixed-latency loops that must not call cudaMalloc after start-up because it can
-// synchronise the device and take unbounded time.  This entry point needs no context, no
-// allocation of any kind (device or host heap): the intermediate field between the axis
-// passes lives in a file-scope __device__ array, and so do the twiddle tables.
+// Who needs it: applications whose device memory is fully reserved up front by another
+// allocator (a framework's caching pool, an MPI+CUDA code that carved HBM at start-up), so
+// that a cudaMalloc would fail, and fixed-latency loops that must not call cudaMalloc after
+// start-up because it can synchronise the device and take unbounded time.  This entry point
+// needs no context and allocates nothing, on the device or on the host heap: the
+// intermediate field between the axis passes lives in a file-scope __device__ array, and so
+// do the twiddle tables, which a small kernel fills on the caller's stream (no host copies).
+// It is still an ordinary CUDA host API call (it queries the device and launches kernels),
+// so it may not be called from a stream callback or a cudaLaunchHostFunc host function,
+// where CUDA calls are not allowed.
 //
 // Limits and sharing rules:
 //   * nx*ny*nz*sizeof(element) <= SMADFT_NOALLOC_MAX_BYTES (16 MiB: 128^3 doubles,
 //     2^22 floats); each length even, at most 512, prime factors 2, 3, 5 only.
 //   * Every GPU that loads the library holds the 16 MiB array (plus 48 KiB of twiddles)
 //     until the process exits.
-//   * All calls share the array, which keeps the last call's contents.  Every element a
-//     call reads from it was written earlier by the same call, so nothing needs clearing;
-//     but calls that overlap on the GPU (different streams, or other host threads on the
-//     same device) race on it.
-//   * The first call on each device looks the array up with cudaGetSymbolAddress while
-//     that device is current; make that first call before any stream capture.
+//   * All calls share the scratch array and the twiddle tables, which keep the last call's
+//     contents.  Every element a call reads from them was written earlier by the same call,
+//     so nothing needs clearing; but calls that overlap on the GPU (different streams, or
+//     other host threads on the same device) race on both.
+//   * The first call on each device looks the arrays up with cudaGetSymbolAddress while
+//     that device is current and sets the kernels' shared-memory attributes; make that
+//     first call before any stream capture.
 //   * The work is queued on `stream` and the call returns without waiting for it.
 #include <cuda_runtime.h>
 
@@ -52,7 +55,7 @@ NaDevice g_na[kNaMaxDevices];
 std::mutex g_na_mu;
 
 // Device addresses of the static arrays for the current device (looked up once per device).
-int na_setup(NaDevice **out)
+int na_setup(NaDevice **out, int *dev_out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
@@ -74,6 +77,7 @@ int na_setup(NaDevice **out)
         d.ready = true;
     }
     *out = &d;
+    *dev_out = dev;
     return SMADFT_OK;
 }
 
@@ -92,8 +96,39 @@ struct NaAxis {
     LinePlan<T> plan;   // radices + device twiddle pointers into g_noalloc_twiddles
 };
 
+// Twiddle tables of the three axes, computed on the device from the lengths alone:
+// w[k] = exp(-2 pi i k / n), h[k] = exp(+i pi k / (2 n)) (the layout LinePlan expects).  One
+// block per axis, FP64 angles through sincospi, queued on the caller's stream.
 template <typename T>
-void na_plan(int n, unsigned char *tw_dev, NaAxis<T> &ax, cpx<T> *host_w, cpx<T> *host_h)
+__global__ void na_twiddle_kernel(unsigned char *tw, int nx, int ny, int nz)
+{
+    const int a = blockIdx.x;
+    const int n = a == 0 ? nx : (a == 1 ? ny : nz);
+    cpx<T> *w = reinterpret_cast<cpx<T> *>(tw + (size_t)a * 2 * kNaMaxLine * 16);
+    cpx<T> *h = w + kNaMaxLine;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double s, c;
+        sincospi(2.0 * (double)k / (double)n, &s, &c);
+        w[k] = {T(c), T(-s)};
+        sincospi((double)k / (2.0 * (double)n), &s, &c);
+        h[k] = {T(c), T(s)};
+    }
+}
+
+// Kernel attributes (dynamic shared memory opt-in) are per device: one flag per device and
+// instantiation, set on the first call under a lock.
+template <class K>
+cudaError_t na_smem_attr(K *kern, size_t smem, int dev, unsigned long long &mask)
+{
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (mask >> dev & 1ull) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) mask |= 1ull << dev;
+    return e;
+}
+
+template <typename T>
+void na_plan(int n, unsigned char *tw_dev, NaAxis<T> &ax)
 {
     ax.n = n;
     ax.plan.n = n;
@@ -104,12 +139,6 @@ void na_plan(int n, unsigned char *tw_dev, NaAxis<T> &ax, cpx<T> *host_w, cpx<T>
     while (m % 5 == 0) { ax.plan.radix[s++] = 5; m /= 5; }
     ax.plan.nst = s;
     for (; s < kMaxStages; s++) ax.plan.radix[s] = 1;
-    for (int k = 0; k < n; k++) {
-        const double a = 2.0 * M_PI * (double)k / (double)n;
-        host_w[k] = {T(std::cos(a)), T(-std::sin(a))};
-        const double b = M_PI * (double)k / (2.0 * (double)n);
-        host_h[k] = {T(std::cos(b)), T(std::sin(b))};
-    }
     ax.plan.w = reinterpret_cast<const cpx<T> *>(tw_dev);
     ax.plan.h = reinterpret_cast<const cpx<T> *>(tw_dev) + kNaMaxLine;
 }
@@ -118,7 +147,7 @@ template <typename T>
 constexpr int na_tile_w() { return sizeof(T) == 4 ? 32 : 16; }
 
 template <typename T, int AXIS>
-cudaError_t na_pass(const Geom &g, const NaAxis<T> &ax, int kind, const T *in, T *out, cudaStream_t st)
+cudaError_t na_pass(const Geom &g, const NaAxis<T> &ax, int kind, const T *in, T *out, cudaStream_t st, int dev)
 {
     LoadArr<T> ld{in};
     StoreArr<T> sv{out};
@@ -134,8 +163,8 @@ cudaError_t na_pass(const Geom &g, const NaAxis<T> &ax, int kind, const T *in, T
 #define SMADFT_NA_CASE(N_)                                                                          \
     case N_: {                                                                                      \
         constexpr size_t smem = fast_smem_bytes<T, N_>();                                           \
-        cudaError_t e = cudaFuncSetAttribute(r2r_fast_kernel<T, N_, AXIS, LoadArr<T>, StoreArr<T>>,  \
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        static unsigned long long mask_ = 0;                                                        \
+        cudaError_t e = na_smem_attr(r2r_fast_kernel<T, N_, AXIS, LoadArr<T>, StoreArr<T>>, smem, dev, mask_); \
         if (e != cudaSuccess) return e;                                                             \
         r2r_fast_kernel<T, N_, AXIS, LoadArr<T>, StoreArr<T>><<<(unsigned)tiles, kFastThreads, smem, st>>>( \
             g, kind, tiles_b, ax.plan.w, ax.plan.h, ld, sv);                                        \
@@ -161,40 +190,31 @@ cudaError_t na_pass(const Geom &g, const NaAxis<T> &ax, int kind, const T *in, T
         a.tiles_b = (g.nz + a.W - 1) / a.W;
         tiles = (long long)(AXIS == 1 ? g.nx : g.ny) * a.tiles_b;
     }
+    // the generic kernel's opt-in is sized for the longest line (one flag per device)
     const size_t smem = 2 * (size_t)(a.W / 2) * a.ld * sizeof(cpx<T>);
-    cudaError_t e = cudaFuncSetAttribute(r2r_pass_kernel<T, LoadArr<T>, StoreArr<T>>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static unsigned long long mask = 0;
+    cudaError_t e = na_smem_attr(r2r_pass_kernel<T, LoadArr<T>, StoreArr<T>>,
+                                 2 * (size_t)(a.W / 2) * kNaMaxLine * sizeof(cpx<T>), dev, mask);
     if (e != cudaSuccess) return e;
     r2r_pass_kernel<T, LoadArr<T>, StoreArr<T>><<<(unsigned)tiles, 256, smem, st>>>(a, ld, sv);
     return cudaGetLastError();
 }
 
 template <typename T>
-int na_transform(const Geom &g, const T *in, T *out, int kx, int ky, int kz, cudaStream_t st, NaDevice &d)
+int na_transform(const Geom &g, const T *in, T *out, int kx, int ky, int kz, cudaStream_t st, NaDevice &d, int dev)
 {
-    // host twiddles on the stack (no heap), uploaded into the static device tables
-    cpx<T> hw[3][kNaMaxLine], hh[3][kNaMaxLine];
     NaAxis<T> ax[3];
     const int lens[3] = {g.nx, g.ny, g.nz};
-    for (int a = 0; a < 3; a++) {
-        unsigned char *tw = d.twiddles + (size_t)a * 2 * kNaMaxLine * 16;
-        na_plan<T>(lens[a], tw, ax[a], hw[a], hh[a]);
-        if (cudaMemcpyAsync(tw, hw[a], sizeof(cpx<T>) * lens[a], cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            cudaMemcpyAsync(tw + sizeof(cpx<T>) * kNaMaxLine, hh[a], sizeof(cpx<T>) * lens[a],
-                            cudaMemcpyHostToDevice, st) != cudaSuccess) {
-            cudaGetLastError();
-            return SMADFT_ERR_CUDA;
-        }
-    }
+    for (int a = 0; a < 3; a++) na_plan<T>(lens[a], d.twiddles + (size_t)a * 2 * kNaMaxLine * 16, ax[a]);
+    na_twiddle_kernel<T><<<3, 256, 0, st>>>(d.twiddles, g.nx, g.ny, g.nz);
+    if (cudaGetLastError() != cudaSuccess) return SMADFT_ERR_CUDA;
     T *tmp = reinterpret_cast<T *>(d.scratch);
-    if (na_pass<T, 2>(g, ax[2], kz, in, tmp, st) != cudaSuccess ||
-        na_pass<T, 1>(g, ax[1], ky, tmp, tmp, st) != cudaSuccess ||
-        na_pass<T, 0>(g, ax[0], kx, tmp, out, st) != cudaSuccess) {
+    if (na_pass<T, 2>(g, ax[2], kz, in, tmp, st, dev) != cudaSuccess ||
+        na_pass<T, 1>(g, ax[1], ky, tmp, tmp, st, dev) != cudaSuccess ||
+        na_pass<T, 0>(g, ax[0], kx, tmp, out, st, dev) != cudaSuccess) {
         cudaGetLastError();
         return SMADFT_ERR_CUDA;
     }
-    // copies from pageable host memory are staged before cudaMemcpyAsync returns, so the
-    // stack twiddle arrays may go out of scope while the work is still queued
     return SMADFT_OK;
 }
 
@@ -212,13 +232,14 @@ extern "C" int smadft_r2r3d_noalloc(const void *in, void *out, int nx, int ny, i
     const size_t es = precision == SMADFT_FP64 ? 8 : 4;
     if ((size_t)nx * ny * nz * es > (size_t)SMADFT_NOALLOC_MAX_BYTES) return SMADFT_ERR_TOO_LARGE;
     NaDevice *d = nullptr;
-    int rc = na_setup(&d);
+    int dev = 0;
+    int rc = na_setup(&d, &dev);
     if (rc) return rc;
     Geom g;
     g.nx = nx; g.ny = ny; g.nz = nz;
     g.nyz = (long long)ny * nz;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (precision == SMADFT_FP64)
-        return na_transform<double>(g, static_cast<const double *>(in), static_cast<double *>(out), kx, ky, kz, st, *d);
-    return na_transform<float>(g, static_cast<const float *>(in), static_cast<float *>(out), kx, ky, kz, st, *d);
+        return na_transform<double>(g, static_cast<const double *>(in), static_cast<double *>(out), kx, ky, kz, st, *d, dev);
+    return na_transform<float>(g, static_cast<const float *>(in), static_cast<float *>(out), kx, ky, kz, st, *d, dev);
 }
