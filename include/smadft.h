@@ -75,6 +75,9 @@ extern "C" {
 #define SMADFT_FIELD_VIRRY 16
 #define SMADFT_FIELD_VIRRZ 17
 #define SMADFT_FIELD_FRHO 18     /* comp: density rate of the last step (its AB2 history)       */
+#define SMADFT_FIELD_DIVV_REAL 19 /* quasi: div v of the last step in real space, scale REDFT01^3
+                                    of SMADFT_FIELD_DIVV (what the reference's save iteration
+                                    writes to divv.dat, quasi/quasi.cpp:2417-2427,2468-2471)      */
 
 /* Interface tracker modes (reference trackers; the scan runs from the last index down) */
 #define SMADFT_TRACK_FLAT 0   /* psi > hi then psi < lo: no-adv/cosNoAdvTrackSing.cpp:880-913  */

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "r2r_fast.cuh"
+#include "r2r_gemm.cuh"
 #include "r2r_plane.cuh"
 #include "r2r_rd.cuh"
 #include "r2r_rdz.cuh"
@@ -53,6 +54,7 @@ struct PlanDev {
     int radix[kMaxStages];
     void *w;   // cpx<T>[n]
     void *h;   // cpx<T>[n]
+    void *gz;  // FP32 contexts, n = 128 / 256: the GEMM-form block matrices of the four kinds
 };
 
 // Model constants handed to device functors by value.
@@ -112,6 +114,9 @@ struct Ctx {
     bool rd_static_kind = true;    // plain strided passes specialised per kind (SMADFT_RD_KIND=0: not)
     bool rd_static_dir = true;     // grouped passes specialised per direction (SMADFT_RD_DIR=0: not)
     bool rdz_stage = true;         // inverse z passes stage their outputs in shared memory (SMADFT_RDZ_STAGE=0: not)
+    bool use_gemm_z = false;       // FP32 plain z passes of length 128 / 256 on the tensor cores (SMADFT_GEMM_Z=1)
+    int num_sms = 148;             // persistent grids (GEMM-form passes): one CTA per SM
+    int *gz_err = nullptr;         // device word: nonzero when a GEMM-form pass gave up a bounded wait
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -343,6 +348,79 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
     }
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link
+// against libcuda)
+using GzEncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+inline GzEncodeFn gz_encode_fn()
+{
+    static GzEncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<GzEncodeFn>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// plain z pass of length N (FP32) in GEMM form on the tensor cores (r2r_gemm.cuh); in == out allowed
+template <int N, bool FWD>
+int launch_gemm_z_k(Ctx &c, int kind, const float *in, float *out)
+{
+    using GI = GzInfo<N>;
+    const int rows = c.g.nx * c.g.ny;
+    const PlanDev &pd = c.plans.at(N);
+    if (!pd.gz || !c.gz_err) {
+        c.err = "GEMM-form z pass: no block matrices for this length";
+        return SMADFT_ERR_STATE;
+    }
+    GzEncodeFn enc = gz_encode_fn();
+    if (!enc) {
+        c.err = "GEMM-form z pass: cuTensorMapEncodeTiled unavailable";
+        return SMADFT_ERR_CUDA;
+    }
+    CUtensorMap map;
+    const cuuint64_t gdim[2] = {(cuuint64_t)N, (cuuint64_t)rows};
+    const cuuint64_t gstride[1] = {(cuuint64_t)N * sizeof(float)};
+    const cuuint32_t box[2] = {32, (cuuint32_t)kGzRows};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(in), gdim, gstride, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        c.err = "GEMM-form z pass: tensor map rejected";
+        return SMADFT_ERR_CUDA;
+    }
+    static unsigned long long attr_set = 0;   // devices whose attribute is set (bit per device)
+    {
+        std::lock_guard<std::mutex> lock(attr_mutex());
+        if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_gemm_z_kernel<N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)GI::SMEM));
+            attr_set |= 1ull << (c.dev % kMaxDevices);
+        }
+    }
+    const int tiles = (rows + kGzRows - 1) / kGzRows;
+    const int grid = tiles < c.num_sms ? tiles : c.num_sms;
+    const __half *mats = reinterpret_cast<const __half *>(pd.gz) + (size_t)kind * GI::MAT_ELEMS;
+    r2r_gemm_z_kernel<N, FWD><<<grid, kGzThreads, GI::SMEM, c.stream>>>(map, out, rows, mats, c.gz_err);
+    SMADFT_CUDA(cudaGetLastError());
+    c.launches++;
+    return SMADFT_OK;
+}
+
+template <int N>
+int launch_gemm_z(Ctx &c, int kind, const float *in, float *out)
+{
+    const bool fwd = kind == K_DCT2 || kind == K_DST2;
+    return fwd ? launch_gemm_z_k<N, true>(c, kind, in, out) : launch_gemm_z_k<N, false>(c, kind, in, out);
+}
+
 // Line lengths with a compile-time staged kernel (the configs' grids); others use the
 // generic one.  Lengths 64/128/256 run the register-direct kernels instead: strided axes
 // with any loader and storer, the z axis for plain arrays.
@@ -363,6 +441,12 @@ int launch_axis(Ctx &c, int kind, LD ld, ST st)
             }
         }
     } else if constexpr (std::is_same<LD, LoadArr<T>>::value && std::is_same<ST, StoreArr<T>>::value) {
+        if constexpr (std::is_same<T, float>::value) {
+            if (c.use_gemm_z && c.gz_err && (n == 128 || n == 256) && ((uintptr_t)ld.p & 15) == 0) {
+                if (n == 256) return launch_gemm_z<256>(c, kind, ld.p, st.p);
+                return launch_gemm_z<128>(c, kind, ld.p, st.p);
+            }
+        }
         if (c.use_rd && c.use_rdz) {
             switch (n) {
             case 64: return launch_rdz<T, 64>(c, kind, ld.p, st.p);

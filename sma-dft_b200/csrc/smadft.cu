@@ -53,6 +53,21 @@ int fail(Ctx &c, int code, const std::string &msg)
     return code;
 }
 
+// After a synchronisation: SMADFT_ERR_TIMEOUT when a GEMM-form pass gave up one of its
+// bounded waits (the error word is cleared again, so the context stays usable).
+int gemm_wait_status(Ctx &c)
+{
+    if (!c.gz_err) return SMADFT_OK;
+    int e = 0;
+    if (cudaMemcpy(&e, c.gz_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, SMADFT_ERR_CUDA, "reading the GEMM-form pass status");
+    }
+    if (!e) return SMADFT_OK;
+    cudaMemset(c.gz_err, 0, sizeof(int));
+    return fail(c, SMADFT_ERR_TIMEOUT, "GEMM-form z pass: a bounded wait ran out (role " + std::to_string(e) + ")");
+}
+
 bool factor_ok(int n)
 {
     if (n < 2 || (n & 1)) return false;
@@ -74,6 +89,54 @@ void make_radices(int n, PlanDev &pd)
     for (; s < kMaxStages; s++) pd.radix[s] = 1;
 }
 
+// FFTW's r2r kinds of length n as dense matrices, Y = M x (unnormalised): REDFT10, REDFT01,
+// RODFT10, RODFT01 in their published definitions.  Angles are reduced exactly in integers
+// (pi a / (2n) with a taken mod 4n) before the FP64 cosine / sine.
+double r2r_matrix_entry(int kind, int n, int k, int m)
+{
+    auto cs = [n](long long a) { return std::cos(M_PI * (double)(a % (4LL * n)) / (2.0 * n)); };
+    auto sn = [n](long long a) { return std::sin(M_PI * (double)(a % (4LL * n)) / (2.0 * n)); };
+    switch (kind) {
+    case K_DCT2: return 2.0 * cs((long long)(2 * m + 1) * k);                      // 2 cos(pi (2m+1) k / 2n)
+    case K_DCT3: return m == 0 ? 1.0 : 2.0 * cs((long long)m * (2 * k + 1));          // x_0 + 2 cos(pi m (2k+1) / 2n)
+    case K_DST2: return 2.0 * sn((long long)(2 * m + 1) * (k + 1));                // 2 sin(pi (2m+1)(k+1) / 2n)
+    default:                                                                          // (-1)^k x_{n-1} + 2 sin(...)
+        return m == n - 1 ? ((k & 1) ? -1.0 : 1.0) : 2.0 * sn((long long)(m + 1) * (2 * k + 1));
+    }
+}
+
+// The GEMM-form z pass's block matrices (r2r_gemm.cuh) of the four kinds, FP16 hi/lo of the
+// entries scaled by 2^12: per kind, NB blocks x {hi, lo} x 128 x 128, row = output index.
+// n = 256 splits each kind by its mirror symmetry: forward kinds take the even / odd output
+// rows over the first 128 inputs (E[k][m] = M[2k][m], O[k][m] = M[2k+1][m]); inverse kinds
+// the even / odd input columns of the first 128 outputs (P[k][j] = M[k][2j],
+// Q[k][j] = M[k][2j+1]).  n = 128 keeps the whole matrix as one block.
+std::vector<__half> gemm_z_matrices(int n)
+{
+    const int nb = n / 128;
+    const size_t per_kind = (size_t)nb * 2 * 128 * 128;
+    std::vector<__half> out(4 * per_kind);
+    for (int kind = 0; kind < 4; kind++) {
+        const bool fwd = kind == K_DCT2 || kind == K_DST2;
+        for (int b = 0; b < nb; b++)
+            for (int r = 0; r < 128; r++)
+                for (int q = 0; q < 128; q++) {
+                    int k = r, m = q;
+                    if (nb == 2) {
+                        if (fwd) k = 2 * r + b;
+                        else m = 2 * q + b;
+                    }
+                    const double v = kGzMatScale * r2r_matrix_entry(kind, n, k, m);
+                    const __half hi = __double2half(v);
+                    const __half lo = __double2half(v - (double)__half2float(hi));
+                    const size_t base = (size_t)kind * per_kind + ((size_t)(2 * b) * 128 + r) * 128 + q;
+                    out[base] = hi;
+                    out[base + 128 * 128] = lo;
+                }
+    }
+    return out;
+}
+
 template <typename T>
 int upload_plan(Ctx &c, int n)
 {
@@ -91,6 +154,11 @@ int upload_plan(Ctx &c, int n)
     SMADFT_CUDA(cudaMalloc(&pd.h, sizeof(cpx<T>) * n));
     SMADFT_CUDA(cudaMemcpy(pd.w, w.data(), sizeof(cpx<T>) * n, cudaMemcpyHostToDevice));
     SMADFT_CUDA(cudaMemcpy(pd.h, h.data(), sizeof(cpx<T>) * n, cudaMemcpyHostToDevice));
+    if (sizeof(T) == 4 && (n == 128 || n == 256)) {
+        const std::vector<__half> m = gemm_z_matrices(n);
+        SMADFT_CUDA(cudaMalloc(&pd.gz, m.size() * sizeof(__half)));
+        SMADFT_CUDA(cudaMemcpy(pd.gz, m.data(), m.size() * sizeof(__half), cudaMemcpyHostToDevice));
+    }
     c.plans[n] = pd;
     return SMADFT_OK;
 }
@@ -241,6 +309,7 @@ int finish_diag(Ctx &c, smadft_diag *out)
     out->mass = ms[0] * dx3;
     out->energy = ms[1] * dx3;
     out->steps = c.steps;
+    if ((rc = gemm_wait_status(c))) return rc;
     return out->nonfinite ? fail(c, SMADFT_ERR_NONFINITE, "psi is not finite") : SMADFT_OK;
 }
 
@@ -435,6 +504,8 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     if (const char *e = std::getenv("SMADFT_RD_KIND")) c.rd_static_kind = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_RD_DIR")) c.rd_static_dir = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_RDZ_STAGE")) c.rdz_stage = e[0] != '0';
+    // SMADFT_GEMM_Z=1: FP32 plain z passes of length 128 / 256 in GEMM form on the tensor cores
+    if (const char *e = std::getenv("SMADFT_GEMM_Z")) c.use_gemm_z = e[0] != '0';
     auto bail = [&](int code) { smadft_destroy(h); return code; };
     if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
@@ -460,6 +531,14 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     }
     rc = c.f32 ? upload_tables<float>(c) : upload_tables<double>(c);
     if (rc) return bail(rc);
+    if (cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.dev) != cudaSuccess || c.num_sms <= 0) {
+        cudaGetLastError();
+        c.num_sms = 148;
+    }
+    if (c.f32) {   // error word of the GEMM-form passes
+        if (cudaMalloc(&c.gz_err, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
+        if (cudaMemset(c.gz_err, 0, sizeof(int)) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+    }
     if ((rc = reduce_init(c))) return bail(rc);
     *out = h;
     return SMADFT_OK;
@@ -474,7 +553,12 @@ int smadft_destroy(smadft_ctx *h)
     for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
     for (int s = 0; s < S_COUNT; s++)
         if (c.slot[s]) cudaFree(c.slot[s]);
-    for (auto &kv : c.plans) { cudaFree(kv.second.w); cudaFree(kv.second.h); }
+    for (auto &kv : c.plans) {
+        cudaFree(kv.second.w);
+        cudaFree(kv.second.h);
+        if (kv.second.gz) cudaFree(kv.second.gz);
+    }
+    if (c.gz_err) cudaFree(c.gz_err);
     if (c.tables64 && c.tables64 != c.tables) cudaFree(c.tables64);
     if (c.tables) cudaFree(c.tables);
     if (c.red) cudaFree(c.red);
@@ -557,6 +641,17 @@ int smadft_get_field(smadft_ctx *h, int field, double *host, size_t n)
     case SMADFT_FIELD_VIRRY: slot = S_VIRY; break;
     case SMADFT_FIELD_VIRRZ: slot = S_VIRZ; break;
     case SMADFT_FIELD_FRHO: slot = S_FRHO; break;
+    case SMADFT_FIELD_DIVV_REAL: {
+        // the reference's save iteration: divv = REDFT01^3(scale divv_hat) (quasi/quasi.cpp:2417-2427)
+        if (c.p.model != SMADFT_MODEL_QUASI) return fail(c, SMADFT_ERR_INVALID, "field not available for this model");
+        int rc = c.f32 ? plain_r2r3d<float>(c, c.f<float>(S_DIVV), c.f<float>(S_TMP), K_DCT3, K_DCT3, K_DCT3)
+                       : plain_r2r3d<double>(c, c.f<double>(S_DIVV), c.f<double>(S_TMP), K_DCT3, K_DCT3, K_DCT3);
+        if (rc) return rc;
+        rc = c.f32 ? get_slot_t<float>(c, S_TMP, host) : get_slot_t<double>(c, S_TMP, host);
+        if (rc) return rc;
+        for (long long q = 0; q < c.n; q++) host[q] *= c.scale;
+        return SMADFT_OK;
+    }
     default: return fail(c, SMADFT_ERR_INVALID, "unknown field");
     }
     if (!c.slot[slot]) return fail(c, SMADFT_ERR_INVALID, "field not available for this model");
@@ -692,7 +787,7 @@ int smadft_sync(smadft_ctx *h)
     Ctx &c = h->c;
     cudaSetDevice(c.dev);
     SMADFT_CUDA(cudaStreamSynchronize(c.stream));
-    return SMADFT_OK;
+    return gemm_wait_status(c);
 }
 
 int smadft_track(smadft_ctx *h, int field, int axis, int mode, double hi, double lo, int *idx,

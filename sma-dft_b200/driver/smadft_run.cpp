@@ -7,6 +7,8 @@
 // energy.dat (quasi/quasi.cpp:2232-2248), info (quasi/quasi.cpp:820-843), and the per-rank
 // text save psi0.dat (adv/cosAdvTrackMult.cpp:1546-1557) which `ic=file:` reads back.
 //
+// quasi also writes the divv.dat, p.dat, rho.dat and energyMid.dat mid slices of its save
+// iteration (quasi/quasi.cpp:91-126,2466-2487).
 // comp (compressible/compressible.cpp) also writes rhoMid.dat and amp.dat mid slices
 // (:2885-2892) and rho0.dat at the end (:2786-2799), and tracks rho > rho_s - 0.15 (:2734).
 //
@@ -151,6 +153,8 @@ int main(int argc, char **argv)
         if (m != SMADFT_MODEL_NOADV) for (const char *f : {"vx.dat", "vy.dat", "vz.dat"}) std::ofstream(out + f).close();
         if (dens) for (const char *f : {"mass.dat", "energy.dat"}) std::ofstream(out + f).close();
         if (m == SMADFT_MODEL_COMP) for (const char *f : {"rhoMid.dat", "amp.dat"}) std::ofstream(out + f).close();
+        if (m == SMADFT_MODEL_QUASI)   // quasi/quasi.cpp:872,926-936
+            for (const char *f : {"divv.dat", "rho.dat", "p.dat", "energyMid.dat"}) std::ofstream(out + f).close();
         std::ofstream info(out + "info");
         info << "Nx: " << p.nx << "\nNy: " << p.ny << "\nNz: " << p.nz << "\nPoints per wavelength (nw): "
              << p.nw << "\nq0 (z direction): " << p.q0 << "\nepsilon: " << p.eps << "\nbeta: " << p.beta
@@ -211,6 +215,16 @@ int main(int argc, char **argv)
                 int ids[2] = {SMADFT_FIELD_RHO, SMADFT_FIELD_AMP};
                 const char *names[2] = {"rhoMid.dat", "amp.dat"};
                 for (int c = 0; c < 2; c++) {
+                    if ((rc = smadft_get_field(ctx, ids[c], field.data(), N))) return die("smadft_get_field", rc, ctx);
+                    append_slice(out + names[c], field, p.nx, p.ny, p.nz);
+                }
+            }
+            if (m == SMADFT_MODEL_QUASI) {
+                // saveMid of div v (real space), pressure, density and energy density at
+                // j = Ny/2 (quasi/quasi.cpp:91-126,2466-2487)
+                int ids[4] = {SMADFT_FIELD_DIVV_REAL, SMADFT_FIELD_P, SMADFT_FIELD_RHO, SMADFT_FIELD_ENERGY};
+                const char *names[4] = {"divv.dat", "p.dat", "rho.dat", "energyMid.dat"};
+                for (int c = 0; c < 4; c++) {
                     if ((rc = smadft_get_field(ctx, ids[c], field.data(), N))) return die("smadft_get_field", rc, ctx);
                     append_slice(out + names[c], field, p.nx, p.ny, p.nz);
                 }

@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(PKG_DIR, "libsmadft.so")
 NOADV, ADV, QUASI, COMP = 0, 1, 2, 3
 FP64, FP32 = 0, 1
 FIELD = dict(psi=0, psihat=1, vx=2, vy=3, vz=4, gx=5, gy=6, gz=7, rho=8, p=9, divv=10, mu=11,
-             energy=12, nhat=13, amp=14, virrx=15, virry=16, virrz=17, frho=18)
+             energy=12, nhat=13, amp=14, virrx=15, virry=16, virrz=17, frho=18, divv_real=19)
 TRACK_FLAT, TRACK_BUMP, TRACK_LEVEL = 0, 1, 2
 REDFT10, REDFT01, RODFT10, RODFT01 = 0, 1, 2, 3
 

@@ -67,7 +67,7 @@ def loss_fd(model, shape, steps, dt, psi0, theta):
 
 CASES = {
     "noadv": (smadft.NOADV, (32, 16, 24), 30, 8, 0.05),
-    "adv": (smadft.ADV, (32, 16, 24), 16, 5, 0.02),
+    "adv": (smadft.ADV, (32, 16, 24), 20, 6, 0.02),
 }
 
 
@@ -114,16 +114,22 @@ def test_autograd_backward_is_the_adjoint(which):
 
 
 def test_autograd_fp32_matches_fp64_through_the_function():
+    """The FP32 adjoint through the function agrees with the FP64 one when both forwards
+    track the same set of interface columns (the loss is piecewise smooth)."""
     model, shape, steps, K, dt = CASES["adv"]
     theta0 = torch.tensor([-0.7, 1.0, 2.0, 1.0, 1.3], dtype=torch.float64)
     psi0_np = smadft.ic_interface(smadft.params(model, shape), A=1.328, bump=0.5 * 2 * np.pi, noise=1e-3,
-                                  seed=43)
-    grads = {}
+                                  seed=31)
+    grads, found = {}, {}
     for prec in (smadft.FP64, smadft.FP32):
         psi0 = torch.tensor(psi0_np, dtype=torch.float64, requires_grad=True)
         theta = theta0.clone().requires_grad_(True)
-        InterfaceLoss.apply(psi0, theta, model, shape, steps, K, dt, prec).backward()
+        out = InterfaceLoss.apply(psi0, theta, model, shape, steps, K, dt, prec)
+        out.backward()
         grads[prec] = (psi0.grad.clone(), theta.grad.clone())
+        found[prec] = out.grad_fn.abi["found"]
+    assert found[smadft.FP32] == found[smadft.FP64]
     (p64, t64), (p32, t32) = grads[smadft.FP64], grads[smadft.FP32]
+    print("theta grad fp64", t64.tolist(), "fp32", t32.tolist())
     assert torch.all(torch.abs(t32 - t64) <= 1e-3 * torch.abs(t64) + 1e-7)
     assert (torch.linalg.norm(p32 - p64) / torch.linalg.norm(p64)).item() <= 1e-3

@@ -103,3 +103,19 @@ def test_autotune_keeps_the_run(model, shape, kw):
     assert len(rep["ms_per_step"]) >= 4          # plane, staged, ungrouped, ... on ny = nz = 64
     assert rep["chosen"] in rep["ms_per_step"]
     assert np.max(np.abs(got - want)) <= 1e-11 * np.max(np.abs(want))
+
+
+def test_autotune_times_the_gemm_form_z_pass_for_fp32():
+    """The tensor-core GEMM-form z pass is an autotuner candidate for FP32 contexts whose z
+    length is 128 or 256 (and only there): it is timed beside the FFT-form paths and kept only
+    when it measures faster."""
+    gemm = "GEMM-form z passes on the tensor cores"
+    for prec, shape, timed in ((smadft.FP32, (8, 32, 256), True), (smadft.FP64, (8, 32, 256), False),
+                               (smadft.FP32, (8, 32, 64), False)):
+        p = smadft.params(smadft.ADV, shape, precision=prec, dt=0.01)
+        with smadft.Solver(p) as s:
+            s.set_psi(ic(p, 5))
+            rep = s.autotune(2)
+            s.step(2)
+            assert np.all(np.isfinite(s.get("psi")))
+        assert (gemm in rep["ms_per_step"]) == timed, (prec, shape, rep)
