@@ -359,57 +359,105 @@ def sweep_params(smadft):
 def run_batch_sweep(torch, smadft, steps, rank, world, dist):
     """Config 4 through smadft_batch: this rank's share of the 48 runs (greedy by cost
     N^3 F, F = 6 noadv / 32 adv), each autotuned, then `steps` batch steps timed with CUDA
-    events on the batch; the same runs stepped one context after another for comparison."""
+    events on the batch stream (members of one model and grid are stepped as groups with
+    pooled fields).  Beside it: the same runs as an FP64 batch (each run's relative L2 error of
+    psi against its FP64 twin after `steps` steps), and 200 steps of the same FP32 runs stepped
+    one context after another and as an ungrouped batch, for comparison."""
     runs = sweep_params(smadft)
     mine = partition_by_cost([n ** 3 * (6 if model == smadft.NOADV else 32) for model, n, _, _ in runs], world, rank)
-    plist = []
-    for i in sorted(mine):
-        model, n, kw, _ = runs[i]
-        plist.append(smadft.params(model, (n, n, n), precision=smadft.FP32, **kw))
+
+    def plist_for(prec):
+        out = []
+        for i in sorted(mine):
+            model, n, kw, _ = runs[i]
+            out.append(smadft.params(model, (n, n, n), precision=prec, **kw))
+        return out
+
     ics = []
-    for (i, p) in zip(sorted(mine), plist):
+    for i, p in zip(sorted(mine), plist_for(smadft.FP32)):
         seed = runs[i][3]
         if p.model == smadft.NOADV:
             ics.append(smadft.ic_interface(p, A=1.328, bump=0.0, noise=1e-3, seed=seed))
         else:
             ics.append(smadft.ic_conics(p, A=1.328, count=4, rmin=1.0, rmax=2.0, noise=1e-3, seed=seed))
+
+    def timed(b, nsteps):
+        stream = torch.cuda.ExternalStream(b.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b.sync()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.step(nsteps)
+        e1.record(stream)
+        b.sync()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
     out = {}
-    with smadft.Batch(plist) as b:
+    with smadft.Batch(plist_for(smadft.FP32)) as b:
         for m, psi in zip(b.members, ics):
             m.set_psi(psi)
         tuned = {}
         for m in b.members:
             rep = m.autotune(2)
             tuned[rep["chosen"]] = tuned.get(rep["chosen"], 0) + 1
+        groups = b.groups
         b.step(3)
+        ms_batch = timed(b, steps)
+        psi32 = [m.get("psi") for m in b.members]
+    with smadft.Batch(plist_for(smadft.FP64)) as b:
+        for m, psi in zip(b.members, ics):
+            m.set_psi(psi)
+        b.step(3 + steps)
         b.sync()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        b.step(steps)
+        psi64 = [m.get("psi") for m in b.members]
+    errs = [float(np.linalg.norm(a - c) / np.linalg.norm(c)) for a, c in zip(psi32, psi64)]
+    finite = all(bool(np.all(np.isfinite(a))) for a in psi32)
+    cmp_steps = min(steps, 200)
+    # the same FP32 runs, one context after another (each on its own graph), and as an
+    # ungrouped batch (each member's own kernels as graph branches)
+    with smadft.Batch(plist_for(smadft.FP32)) as b:
+        for m, psi in zip(b.members, ics):
+            m.set_psi(psi)
+            m.step(3)
         b.sync()
-        ms_batch = 1000.0 * (time.perf_counter() - t0)
-        finite = all(bool(np.all(np.isfinite(m.get("psi")))) for m in b.members)
-        # the same members stepped one after another (each on its own graph)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for m in b.members:
-            m.step(steps)
+            m.step(cmp_steps)
         for m in b.members:
             m.sync()
         ms_solo = 1000.0 * (time.perf_counter() - t0)
+    os.environ["SMADFT_BATCH_GROUP"] = "0"
+    try:
+        with smadft.Batch(plist_for(smadft.FP32)) as b:
+            for m, psi in zip(b.members, ics):
+                m.set_psi(psi)
+            b.step(3)
+            ms_ungrouped = timed(b, cmp_steps)
+    finally:
+        del os.environ["SMADFT_BATCH_GROUP"]
+    bytes_per_step = sum(4.0 * n ** 3 * (6 if model == smadft.NOADV else 32)
+                         for i, (model, n, _, _) in enumerate(runs) if i in set(mine))
     if world > 1:
-        ms_batch, ms_solo = max_over_ranks(torch, dist, [ms_batch, ms_solo], "cuda")
+        ms_batch, ms_solo, ms_ungrouped = max_over_ranks(torch, dist, [ms_batch, ms_solo, ms_ungrouped], "cuda")
         c = torch.tensor([float(finite)], device="cuda")
         dist.all_reduce(c, op=dist.ReduceOp.MIN)
         finite = bool(c.item())
     total = len(runs) * steps
-    out = {"runs": len(runs), "runs_on_rank0": len(plist), "steps": steps,
+    out = {"runs": len(runs), "runs_on_rank0": len(psi32), "steps": steps,
            "grids": "12 each of 64^3, 96^3, 128^3, 160^3; noadv/adv alternating; FP32",
+           "groups_rank0": groups,
            "aggregate_steps_per_s": total / (ms_batch / 1000.0),
            "ms_per_batch_step": ms_batch / steps,
-           "sequential_aggregate_steps_per_s": total / (ms_solo / 1000.0),
+           "hbm_frac_rank0": bytes_per_step / (ms_batch / steps * 1e-3) / 1e9 / peaks()[0],
+           "sequential_aggregate_steps_per_s": len(runs) * cmp_steps / (ms_solo / 1000.0),
+           "ungrouped_batch_aggregate_steps_per_s": len(runs) * cmp_steps / (ms_ungrouped / 1000.0),
+           "comparison_steps": cmp_steps,
+           "rel_l2_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)),
+                                  "per_run": [float(f"{e:.3e}") for e in errs]},
            "autotuned_paths_rank0": tuned, "finite": finite,
-           "timing": "host wall clock around batch_step + sync, max over ranks"}
+           "timing": "CUDA events on the batch stream (sequential: host wall clock), max over ranks"}
     return out
 
 
@@ -609,10 +657,11 @@ def run_ours(args, rank, world, local_rank):
 def run_kernel_only(args):
     """A few launches of one kernel family for profiling (ncu): no timing, no JSON.
 
-    pass-z | pass-y | pass-x: one plain DCT-II axis pass on a 256^3 field (2 fields held).
+    pass-z | pass-y | pass-x: one plain axis pass (kind --kind) on a 256^3 field (2 fields held).
     r2r3d: one plain 3-D DCT-III (the plane kernel for z and y where it applies, then x).
     step: loop bodies of the adv model (all its kernels).
     comp-step: loop bodies of the compressible model past its relaxation switch.
+    batch-step: config 4's 48-run FP32 batch, one eager body and `reps` graph-replayed bodies.
     """
     import torch
     import smadft
@@ -627,7 +676,7 @@ def run_kernel_only(args):
             torch.cuda.synchronize()
             axis = {"pass-z": 2, "pass-y": 1, "pass-x": 0}[args.kernel_only]
             for _ in range(args.reps):
-                s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, 0)
+                s.r2r_pass_device(x.data_ptr(), y.data_ptr(), axis, args.kind)
         elif args.kernel_only == "r2r3d":
             dt = torch.float32 if prec == smadft.FP32 else torch.float64
             x = torch.randn((n, n, n), device="cuda", dtype=dt)
@@ -640,6 +689,16 @@ def run_kernel_only(args):
             s.set_psi(smadft.ic_conics(p2, A=1.328, count=4, rmin=3.0, rmax=6.0, seed=1))
             s.step(args.reps)
         s.sync()
+    if args.kernel_only == "batch-step":
+        # config 4's 48 FP32 runs (grouped batch): set-up, one eager body, then `reps` graph bodies
+        plist = [smadft.params(model, (nn, nn, nn), precision=smadft.FP32, **kw)
+                 for model, nn, kw, _ in sweep_params(smadft)]
+        with smadft.Batch(plist) as b:
+            for m, p2 in zip(b.members, plist):
+                m.set_psi(smadft.ic_interface(p2, A=1.328, bump=0.0, noise=1e-3, seed=1))
+            b.step(1)
+            b.step(args.reps)
+            b.sync()
     if args.kernel_only == "comp-step":
         pc = smadft.params(smadft.COMP, (n, n, n), precision=prec, divv_switch=1)
         x = np.arange(n)[:, None, None]
@@ -659,17 +718,20 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--sweep-steps", type=int, default=200,
-                    help="steps of the 48-run batched sweep (config 4 runs 2000; 0: skip)")
+    ap.add_argument("--sweep-steps", type=int, default=2000,
+                    help="steps of the 48-run batched sweep (config 4: 2000; 0: skip)")
     ap.add_argument("--err-steps", type=int, default=ERR_STEPS,
                     help="steps after which the FP32 error against FP64 is reported (0: after the timed steps)")
-    ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "r2r3d", "step", "comp-step"], default=None,
+    ap.add_argument("--kernel-only", choices=["pass-z", "pass-y", "pass-x", "r2r3d", "step", "comp-step", "batch-step"],
+                    default=None,
                     help="launch one kernel family a few times (for profilers) and exit")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--adjoint-steps", type=int, default=500,
                     help="steps of the 128^3 adv adjoint measurement (0: skip)")
     ap.add_argument("--shape", type=int, default=N)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--kind", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="kernel-only passes: 0 DCT-II, 1 DCT-III, 2 DST-II, 3 DST-III")
     args = ap.parse_args()
     if args.kernel_only:
         return run_kernel_only(args)

@@ -238,6 +238,10 @@ int smadft_r2r3d_noalloc(const void *in, void *out, int nx, int ny, int nz, int 
  * the reference runs each as its own MPI job.  A batch owns n contexts (any model, grid,
  * precision and parameters; one device); smadft_batch_step advances every member by nsteps
  * loop bodies, each body one CUDA graph that runs all members' kernels concurrently.
+ * Members of the same model (noadv or adv, non-conserved), grid and precision form a group:
+ * their fields share one allocation per field, and each plain axis pass of the group runs as
+ * one launch over all of them (the passes that carry a member's parameters run per member);
+ * SMADFT_BATCH_GROUP=0 in the environment turns grouping off.
  * Members are ordinary contexts for everything else (smadft_batch_member): set their
  * initial conditions, read fields, track, checkpoint.  A batch is not thread-safe. */
 typedef struct smadft_batch smadft_batch;
@@ -247,6 +251,11 @@ int smadft_batch_size(const smadft_batch *batch, int *n);
 int smadft_batch_member(smadft_batch *batch, int i, smadft_ctx **ctx);
 int smadft_batch_step(smadft_batch *batch, int nsteps);
 int smadft_batch_sync(smadft_batch *batch);
+/* The batch's CUDA stream (a cudaStream_t): every batch step is ordered on it, so callers can
+ * time or order work around smadft_batch_step. */
+int smadft_batch_get_stream(smadft_batch *batch, void **stream);
+/* Number of member groups advanced with pooled fields (see above). */
+int smadft_batch_groups(const smadft_batch *batch, int *groups);
 const char *smadft_batch_last_error(const smadft_batch *batch);
 
 /* ---- adjoint (diffusive and advected models) -------------------------------------------

@@ -18,6 +18,7 @@
 #include "r2r_plane.cuh"
 #include "r2r_rd.cuh"
 #include "r2r_rdz.cuh"
+#include "r2r_rdt.cuh"
 #include "r2r_pass.cuh"
 #include "smadft.h"
 
@@ -117,6 +118,9 @@ struct Ctx {
     bool use_gemm_z = false;       // FP32 plain z passes of length 128 / 256 on the tensor cores (SMADFT_GEMM_Z=1)
     int num_sms = 148;             // persistent grids (GEMM-form passes): one CTA per SM
     int *gz_err = nullptr;         // device word: nonzero when a GEMM-form pass gave up a bounded wait
+    bool use_tma = false;          // FP32 plain strided passes fed by TMA, persistent (SMADFT_TMA_PASS=1)
+    int grid_y = 1;                // strided and generic passes: CTA rows (fields of a batch group, LoadArrM)
+    bool pooled = false;           // field slots live in a batch group's pools (the batch frees them)
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -213,7 +217,7 @@ int launch_generic(Ctx &c, int axis, int kind, LD ld, ST st)
             attr_set[c.dev % kMaxDevices] = smem;
         }
     }
-    r2r_pass_kernel<T, LD, ST><<<(unsigned)tiles, 256, smem, c.stream>>>(a, ld, st);
+    r2r_pass_kernel<T, LD, ST><<<dim3((unsigned)tiles, (unsigned)c.grid_y), 256, smem, c.stream>>>(a, ld, st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
     return SMADFT_OK;
@@ -235,7 +239,8 @@ int launch_rd_k(Ctx &c, const KindSet<NC> &kinds, LD ld, ST st)
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND, DIR><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+    r2r_rd_kernel<T, N, AXIS, LD, ST, NC, KIND, DIR><<<dim3((unsigned)tiles, (unsigned)c.grid_y), RdInfo<N>::THREADS, smem,
+                                                       c.stream>>>(
         c.g, kinds, tiles_b, ld, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
@@ -299,7 +304,7 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_fast_kernel<T, N, AXIS, LD, ST, CFG><<<(unsigned)tiles, CFG::THREADS, smem, c.stream>>>(
+    r2r_fast_kernel<T, N, AXIS, LD, ST, CFG><<<dim3((unsigned)tiles, (unsigned)c.grid_y), CFG::THREADS, smem, c.stream>>>(
         c.g, kind, tiles_b, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h), ld, st);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
@@ -369,6 +374,58 @@ inline GzEncodeFn gz_encode_fn()
     return fn;
 }
 
+// plain FP32 strided pass of length N fed by TMA (r2r_rdt.cuh): persistent, two CTAs per SM
+template <int N, int AXIS, class ST, int KIND>
+int launch_rdt_k(Ctx &c, int kind, const float *in, ST st)
+{
+    const int tiles_b = (c.g.nz + 31) / 32;
+    const int tiles = (AXIS == 1 ? c.g.nx : c.g.ny) * tiles_b;
+    GzEncodeFn enc = gz_encode_fn();
+    if (!enc) {
+        c.err = "TMA-fed pass: cuTensorMapEncodeTiled unavailable";
+        return SMADFT_ERR_CUDA;
+    }
+    CUtensorMap map;
+    const cuuint64_t gdim[3] = {(cuuint64_t)c.g.nz, (cuuint64_t)c.g.ny, (cuuint64_t)c.g.nx};
+    const cuuint64_t gstride[2] = {(cuuint64_t)c.g.nz * sizeof(float), (cuuint64_t)c.g.nyz * sizeof(float)};
+    const cuuint32_t box[3] = {32, AXIS == 1 ? (cuuint32_t)N : 1u, AXIS == 0 ? (cuuint32_t)N : 1u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(in), gdim, gstride, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        c.err = "TMA-fed pass: tensor map rejected";
+        return SMADFT_ERR_CUDA;
+    }
+    constexpr size_t smem = rdt_smem_bytes<float, float, N>();
+    static unsigned long long attr_set = 0;
+    {
+        std::lock_guard<std::mutex> lock(attr_mutex());
+        if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdt_kernel<float, float, N, AXIS, ST, KIND>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr_set |= 1ull << (c.dev % kMaxDevices);
+        }
+    }
+    const PlanDev &pd = c.plans.at(N);
+    const int grid = tiles < 2 * c.num_sms ? tiles : 2 * c.num_sms;
+    r2r_rdt_kernel<float, float, N, AXIS, ST, KIND><<<grid, RdInfo<N>::THREADS, smem, c.stream>>>(
+        map, c.g, kind, tiles, tiles_b, reinterpret_cast<const cpx<float> *>(pd.w),
+        reinterpret_cast<const cpx<float> *>(pd.h), st, c.gz_err);
+    SMADFT_CUDA(cudaGetLastError());
+    c.launches++;
+    return SMADFT_OK;
+}
+
+template <int N, int AXIS, class ST>
+int launch_rdt(Ctx &c, int kind, const float *in, ST st)
+{
+    switch (kind) {
+    case K_DCT2: return launch_rdt_k<N, AXIS, ST, K_DCT2>(c, kind, in, st);
+    case K_DCT3: return launch_rdt_k<N, AXIS, ST, K_DCT3>(c, kind, in, st);
+    default: return launch_rdt_k<N, AXIS, ST, -1>(c, kind, in, st);
+    }
+}
+
 // plain z pass of length N (FP32) in GEMM form on the tensor cores (r2r_gemm.cuh); in == out allowed
 template <int N, bool FWD>
 int launch_gemm_z_k(Ctx &c, int kind, const float *in, float *out)
@@ -431,6 +488,17 @@ template <typename T, int AXIS, class LD, class ST>
 int launch_axis(Ctx &c, int kind, LD ld, ST st)
 {
     const int n = AXIS == 0 ? c.g.nx : (AXIS == 1 ? c.g.ny : c.g.nz);
+    if constexpr (AXIS != 2 && std::is_same<T, float>::value && std::is_same<LD, LoadArr<float>>::value) {
+        // plain FP32 inputs: the TMA-fed persistent pass where enabled and the layout allows
+        if (c.use_tma && c.gz_err && c.grid_y == 1 && c.g.nz % 4 == 0 && ((uintptr_t)ld.p & 15) == 0) {
+            switch (n) {
+            case 64: return launch_rdt<64, AXIS>(c, kind, ld.p, st);
+            case 128: return launch_rdt<128, AXIS>(c, kind, ld.p, st);
+            case 256: return launch_rdt<256, AXIS>(c, kind, ld.p, st);
+            default: break;
+            }
+        }
+    }
     if constexpr (AXIS != 2) {
         if (c.use_rd) {
             switch (n) {
@@ -605,6 +673,75 @@ int forked(Ctx &c, int n, F fn)
         return SMADFT_ERR_CUDA;
     }
     return SMADFT_OK;
+}
+
+// ---- batch groups: M members of one model and grid whose fields lie in pools (member i's
+// field at the lead's pointer + i n elements).  Their plain axis passes run as one launch over
+// the pool; passes with member-specific loaders or storers run per member on the lead's stream.
+
+// `fn` on a copy of the lead context (same stream, plans and launch helpers) whose geometry
+// or grid is widened to the whole pool; the copy's launches are counted on the lead
+template <class F>
+int on_pool_copy(Ctx &lead, F fn)
+{
+    Ctx pc = lead;
+    const int rc = fn(pc);
+    lead.launches = pc.launches;
+    if (rc) lead.err = pc.err;
+    return rc;
+}
+
+// one plain axis pass over the pooled fields of M members: z and y passes see the pool as one
+// field of M nx planes; x passes run M CTA rows, each addressing its member's field
+template <typename T, int AXIS, typename S = T>
+int pooled_pass(Ctx &lead, int M, int kind, const S *in, T *out)
+{
+    return on_pool_copy(lead, [&](Ctx &pc) {
+        if constexpr (AXIS == 0) {
+            pc.grid_y = M;
+            return launch_axis<T, 0>(pc, kind, LoadArrM<T, S>{in, (idx_t)lead.n}, StoreArrM<T>{out, (idx_t)lead.n});
+        } else {
+            pc.g.nx = lead.g.nx * M;
+            return launch_axis<T, AXIS>(pc, kind, LoadArr<T, S>{in}, StoreArr<T>{out});
+        }
+    });
+}
+
+// the y passes of NC components with loaders ls (one grouped launch where the length has the
+// register-direct kernel, else one pass per component), outputs into out[m]
+template <typename T, int NC, int DIR, class... L>
+int y_pass_multi(Ctx &c, const int (&ky)[NC], T *const (&out)[NC], L... ls)
+{
+    static_assert(sizeof...(L) == NC, "one loader per component");
+    if (c.g.ny == 64 || c.g.ny == 128 || c.g.ny == 256) {
+        KindSet<NC> ks;
+        StoreMulti<T, NC> sm;
+        for (int m = 0; m < NC; m++) {
+            ks.k[m] = ky[m];
+            sm.p[m] = out[m];
+        }
+        using LM = decltype(make_multi(ls...));
+        using SM = StoreMulti<T, NC>;
+        switch (c.g.ny) {
+        case 64: return launch_rd<T, 64, 1, LM, SM, NC, DIR>(c, ks, make_multi(ls...), sm);
+        case 128: return launch_rd<T, 128, 1, LM, SM, NC, DIR>(c, ks, make_multi(ls...), sm);
+        default: return launch_rd<T, 256, 1, LM, SM, NC, DIR>(c, ks, make_multi(ls...), sm);
+        }
+    }
+    int rc = SMADFT_OK, m = 0;
+    ((rc = rc ? rc : launch_axis<T, 1>(c, ky[m], ls, StoreArr<T>{out[m]}), m++), ...);
+    return rc;
+}
+
+// runs fn(member) with the member's launches on the lead's stream
+template <class F>
+int on_lead_stream(Ctx &lead, Ctx &member, F fn)
+{
+    const cudaStream_t own = member.stream;
+    member.stream = lead.stream;
+    const int rc = fn(member);
+    member.stream = own;
+    return rc;
 }
 
 // NC 3-D transforms whose loaders share input fields: component m goes from loader ls[m]

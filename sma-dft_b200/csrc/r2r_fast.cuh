@@ -5,7 +5,8 @@
 //   * the tile (W = 32 lines) is staged once in shared memory as 16 complex lines
 //     (two real lines per complex line, Makhoul permutation applied on the way in);
 //   * the complex FFT is an in-place mixed-radix decimation-in-frequency with register
-//     codelets of radix 16/8/4/2/3/5 (e.g. 256 = 16 x 16: two passes over shared memory);
+//     codelets of radix 16/10/8/6/4/2/3/5 (e.g. 256 = 16 x 16, 160 = 16 x 10, 96 = 16 x 6:
+//     two passes over shared memory);
 //     its output is left in digit-reversed order and read back through that map;
 //   * shared-memory positions are padded (one slot per last-radix block, one per line)
 //     so the stage loads/stores and the row-major global staging are bank-conflict free;
@@ -32,9 +33,9 @@ SMADFT_PLAN(40, 2, 8, 5, 1)
 SMADFT_PLAN(48, 2, 16, 3, 1)
 SMADFT_PLAN(64, 2, 8, 8, 1)
 SMADFT_PLAN(80, 2, 16, 5, 1)
-SMADFT_PLAN(96, 3, 16, 3, 2)
+SMADFT_PLAN(96, 2, 16, 6, 1)
 SMADFT_PLAN(128, 2, 16, 8, 1)
-SMADFT_PLAN(160, 3, 16, 5, 2)
+SMADFT_PLAN(160, 2, 16, 10, 1)
 SMADFT_PLAN(192, 3, 16, 4, 3)
 SMADFT_PLAN(256, 2, 16, 16, 1)
 SMADFT_PLAN(320, 3, 16, 4, 5)
@@ -123,6 +124,37 @@ __device__ __forceinline__ void codelet(cpx<T> *v)
         dft<R, T, INV>(v);
     } else if constexpr (R == 4) {
         dft4<T, INV>(v[0], v[1], v[2], v[3]);
+    } else if constexpr (R == 6 || R == 10) {
+        // radix-2 decimation in time over two length-R/2 DFTs (R/2 = 3 or 5):
+        // X[k] = E[k] + w^k O[k], X[k + R/2] = E[k] - w^k O[k], w = exp(-+ 2 pi i / R)
+        constexpr int H = R / 2;
+        cpx<T> e[H], o[H];
+#pragma unroll
+        for (int m = 0; m < H; m++) {
+            e[m] = v[2 * m];
+            o[m] = v[2 * m + 1];
+        }
+        dft<H, T, INV>(e);
+        dft<H, T, INV>(o);
+#pragma unroll
+        for (int k = 0; k < H; k++) {
+            cpx<T> t = o[k];
+            if (k > 0) {
+                T c, sn;   // cos, sin of 2 pi k / R
+                if constexpr (R == 6) {
+                    c = k == 1 ? T(0.5) : T(-0.5);
+                    sn = T(0.86602540378443864676372317075294);
+                } else {
+                    const T c1 = T(0.80901699437494742410229341718282), s1 = T(0.58778525229247312916870595463907);
+                    const T c2 = T(0.30901699437494742410229341718282), s2 = T(0.95105651629515357211643933337938);
+                    c = k == 1 ? c1 : k == 2 ? c2 : k == 3 ? -c2 : -c1;
+                    sn = (k == 1 || k == 4) ? s1 : s2;
+                }
+                t = cmul(t, cpx<T>{c, INV ? sn : -sn});
+            }
+            v[k] = cadd(e[k], t);
+            v[k + H] = csub(e[k], t);
+        }
     } else if constexpr (R == 8) {
         // radix-2 decimation in time over two length-4 DFTs
         cpx<T> e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};

@@ -168,6 +168,38 @@ struct StoreArr {
     __device__ __forceinline__ void store(idx_t idx, int, int, int, const T *v) const { vst_as<T, V, S>(p, idx, v); }
 };
 
+// The same for M equal fields laid out one after another, n elements apart (the pooled
+// fields of a batch group): CTA row blockIdx.y works on field blockIdx.y, so one launch with
+// gridDim.y = M runs an axis pass over all M fields.
+template <typename T, typename S = T>
+struct LoadArrM {
+    const S *__restrict__ p;
+    idx_t n;
+    template <int V>
+    __device__ __forceinline__ void load(idx_t idx, int, int, int, T *out) const
+    {
+        vld_as<T, V, S>(p + (size_t)blockIdx.y * n, idx, out);
+    }
+};
+template <typename T, typename S = T>
+struct StoreArrM {
+    S *__restrict__ p;
+    idx_t n;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(idx_t, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void fin(idx_t idx, int, int, int, const T *v, const T *) const
+    {
+        vst_as<T, V, S>(p + (size_t)blockIdx.y * n, idx, v);
+    }
+    template <int V>
+    __device__ __forceinline__ void store(idx_t idx, int, int, int, const T *v) const
+    {
+        vst_as<T, V, S>(p + (size_t)blockIdx.y * n, idx, v);
+    }
+};
+
 template <class ST, typename T, class = void>
 struct pre_type { using type = T; };
 template <class ST, typename T>

@@ -506,6 +506,8 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     if (const char *e = std::getenv("SMADFT_RDZ_STAGE")) c.rdz_stage = e[0] != '0';
     // SMADFT_GEMM_Z=1: FP32 plain z passes of length 128 / 256 in GEMM form on the tensor cores
     if (const char *e = std::getenv("SMADFT_GEMM_Z")) c.use_gemm_z = e[0] != '0';
+    // SMADFT_TMA_PASS=1: FP32 plain strided passes fed by TMA (r2r_rdt.cuh)
+    if (const char *e = std::getenv("SMADFT_TMA_PASS")) c.use_tma = e[0] != '0';
     auto bail = [&](int code) { smadft_destroy(h); return code; };
     if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
@@ -552,7 +554,7 @@ int smadft_destroy(smadft_ctx *h)
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
     for (int s = 0; s < S_COUNT; s++)
-        if (c.slot[s]) cudaFree(c.slot[s]);
+        if (c.slot[s] && !c.pooled) cudaFree(c.slot[s]);
     for (auto &kv : c.plans) {
         cudaFree(kv.second.w);
         cudaFree(kv.second.h);

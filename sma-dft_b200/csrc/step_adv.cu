@@ -76,15 +76,111 @@ int adv_step(Ctx &c)
                     LdAdvN<T>{psi, vx, vy, vz, gx, gy, gz, s.beta, s.gamma}, StUpdCN<T>{make_spec<double>(c), ph, np});
 }
 
+// The same loop body for M batch members of one grid whose fields are pooled (member i's
+// slot = the lead's slot + i n elements): per transform, the y passes with each member's
+// loaders (its own parameters) run per member; the plain z and x passes run once over the
+// pool; the CN/AB2 x pass runs per member (its storer carries the member's parameters).  All
+// launches go to the lead's stream.  Non-conserved runs only.
+template <typename T>
+int adv_group_step(Ctx *const *mm, int M)
+{
+    Ctx &L = *mm[0];
+    int rc;
+    auto pz = [&](int slot, int kind) { return pooled_pass<T, 2>(L, M, kind, L.f<T>(slot), L.f<T>(slot)); };
+    auto px = [&](int slot, int kind) { return pooled_pass<T, 0>(L, M, kind, L.f<T>(slot), L.f<T>(slot)); };
+    // psi, grad psi and Sp2 from psihat (adv/cosAdvTrackMult.cpp:904-991)
+    {
+        const int kx[5] = {K_DCT3, K_DST3, K_DCT3, K_DCT3, K_DCT3};
+        const int ky[5] = {K_DCT3, K_DCT3, K_DST3, K_DCT3, K_DCT3};
+        const int kz[5] = {K_DCT3, K_DCT3, K_DCT3, K_DST3, K_DCT3};
+        const int slots[5] = {S_PSI, S_GX, S_GY, S_GZ, S_SP2};
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                Spec<T> s = make_spec<T>(c);
+                double *ph = c.f<double>(S_PSIH);
+                T *const out[5] = {c.f<T>(S_PSI), c.f<T>(S_GX), c.f<T>(S_GY), c.f<T>(S_GZ), c.f<T>(S_SP2)};
+                return y_pass_multi<T, 5, 0>(c, ky, out, LoadArr<T, double>{ph}, LdGrad<T, 0, double>{s, ph},
+                                             LdGrad<T, 1, double>{s, ph}, LdGrad<T, 2, double>{s, ph},
+                                             LdNegLin<T>{s, ph});
+            });
+            if (rc) return rc;
+        }
+        for (int m = 0; m < 5; m++)
+            if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
+    }
+    // force spectra S_c = ST_c(mu d_c psi) (:996-1027)
+    {
+        const int kx[3] = {K_DST2, K_DCT2, K_DCT2};
+        const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
+        const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
+        const int slots[3] = {S_SX, S_SY, S_SZ};
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                Spec<T> s = make_spec<T>(c);
+                T *psi = c.f<T>(S_PSI), *sp2 = c.f<T>(S_SP2);
+                T *const out[3] = {c.f<T>(S_SX), c.f<T>(S_SY), c.f<T>(S_SZ)};
+                return y_pass_multi<T, 3, 1>(c, ky, out, LdForce<T>{psi, sp2, c.f<T>(S_GX), s.beta, s.gamma},
+                                             LdForce<T>{psi, sp2, c.f<T>(S_GY), s.beta, s.gamma},
+                                             LdForce<T>{psi, sp2, c.f<T>(S_GZ), s.beta, s.gamma});
+            });
+            if (rc) return rc;
+        }
+        for (int m = 0; m < 3; m++)
+            if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
+    }
+    // Stokes velocity (:1030-1286)
+    {
+        const int kx[3] = {K_DST3, K_DCT3, K_DCT3};
+        const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
+        const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
+        const int slots[3] = {S_VX, S_VY, S_VZ};
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                Spec<T> s = make_spec<T>(c);
+                T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
+                T *const out[3] = {c.f<T>(S_VX), c.f<T>(S_VY), c.f<T>(S_VZ)};
+                return y_pass_multi<T, 3, 0>(c, ky, out, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr},
+                                             LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr},
+                                             LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr});
+            });
+            if (rc) return rc;
+        }
+        for (int m = 0; m < 3; m++)
+            if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
+    }
+    // N = beta psi^3 - gamma psi^5 - v.grad psi into the scratch field, CN/AB2 update (:1290-1365)
+    for (int i = 0; i < M; i++) {
+        rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+            Spec<T> s = make_spec<T>(c);
+            return launch_axis<T, 1>(c, K_DCT2,
+                                     LdAdvN<T>{c.f<T>(S_PSI), c.f<T>(S_VX), c.f<T>(S_VY), c.f<T>(S_VZ), c.f<T>(S_GX),
+                                               c.f<T>(S_GY), c.f<T>(S_GZ), s.beta, s.gamma},
+                                     StoreArr<T>{c.f<T>(S_TMP)});
+        });
+        if (rc) return rc;
+    }
+    if ((rc = pz(S_TMP, K_DCT2))) return rc;
+    for (int i = 0; i < M; i++) {
+        rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+            return launch_axis<T, 0>(c, K_DCT2, LoadArr<T>{c.f<T>(S_TMP)},
+                                     StUpdCN<T>{make_spec<double>(c), c.f<double>(S_PSIH), c.f<T>(S_NP)});
+        });
+        if (rc) return rc;
+    }
+    return SMADFT_OK;
+}
+
 // each precision builds as its own object (SMADFT_INST_FLOAT / SMADFT_INST_DOUBLE); a plain
 // compile without either instantiates both
 #if !defined(SMADFT_INST_DOUBLE)
 template int adv_fields<float>(Ctx &);
 template int adv_step<float>(Ctx &);
+template int adv_group_step<float>(Ctx *const *, int);
 #endif
 #if !defined(SMADFT_INST_FLOAT)
 template int adv_fields<double>(Ctx &);
 template int adv_step<double>(Ctx &);
+template int adv_group_step<double>(Ctx *const *, int);
 #endif
 
 }  // namespace smadft

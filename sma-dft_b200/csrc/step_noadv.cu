@@ -24,6 +24,35 @@ int noadv_step(Ctx &c, bool keep_old)
     return r2r3d<T>(c, K_DCT3, K_DCT3, K_DCT3, LoadArr<T, double>{ph}, StoreArr<T>{dst});
 }
 
+// The diffusive loop body for M batch members of one grid with pooled fields (see
+// adv_group_step): per member the nonlinearity's y pass and the CN/AB2 x pass (their
+// functors carry the member's parameters), the plain passes once over the pool.
+template <typename T>
+int noadv_group_step(Ctx *const *mm, int M)
+{
+    Ctx &L = *mm[0];
+    int rc;
+    for (int i = 0; i < M; i++) {
+        rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+            Spec<T> s = make_spec<T>(c);
+            return launch_axis<T, 1>(c, K_DCT2, LdNonlin<T>{c.f<T>(S_PSI), s.beta, s.gamma}, StoreArr<T>{c.f<T>(S_TMP)});
+        });
+        if (rc) return rc;
+    }
+    if ((rc = pooled_pass<T, 2>(L, M, K_DCT2, L.f<T>(S_TMP), L.f<T>(S_TMP)))) return rc;
+    for (int i = 0; i < M; i++) {
+        rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+            return launch_axis<T, 0>(c, K_DCT2, LoadArr<T>{c.f<T>(S_TMP)},
+                                     StUpdCN<T>{make_spec<double>(c), c.f<double>(S_PSIH), c.f<T>(S_NP)});
+        });
+        if (rc) return rc;
+    }
+    // psi^{n+1} = REDFT01^3 psihat, all members at once
+    if ((rc = pooled_pass<T, 1, double>(L, M, K_DCT3, L.f<double>(S_PSIH), L.f<T>(S_TMP)))) return rc;
+    if ((rc = pooled_pass<T, 2>(L, M, K_DCT3, L.f<T>(S_TMP), L.f<T>(S_TMP)))) return rc;
+    return pooled_pass<T, 0>(L, M, K_DCT3, L.f<T>(S_TMP), L.f<T>(S_PSI));
+}
+
 template <typename T>
 int refresh_psi(Ctx &c, T *dst)
 {
@@ -85,7 +114,8 @@ int plain_pass(Ctx &c, const T *in, T *out, int axis, int kind)
     template int dfd_field<T>(Ctx &, T *);                                 \
     template int psihat_from_psi<T>(Ctx &);                                \
     template int plain_r2r3d<T>(Ctx &, const T *, T *, int, int, int);     \
-    template int plain_pass<T>(Ctx &, const T *, T *, int, int);
+    template int plain_pass<T>(Ctx &, const T *, T *, int, int);          \
+    template int noadv_group_step<T>(Ctx *const *, int);
 // each precision builds as its own object (SMADFT_INST_FLOAT / SMADFT_INST_DOUBLE); a plain
 // compile without either instantiates both
 #if !defined(SMADFT_INST_DOUBLE)

@@ -10,6 +10,10 @@ namespace smadft {
 template <typename T> int noadv_step(Ctx &c, bool keep_old);
 // adv/cosAdvTrackMult.cpp:824-1369,1742
 template <typename T> int adv_step(Ctx &c);
+// the noadv / adv loop bodies of M batch members of one model and grid whose fields are
+// pooled (member i's slot = mm[0]'s slot + i n elements), all on mm[0]'s stream; non-conserved
+template <typename T> int noadv_group_step(Ctx *const *mm, int M);
+template <typename T> int adv_group_step(Ctx *const *mm, int M);
 // its first part (:847-1286): psi, grad psi, Sp2, S-hat and v from psihat into their slots
 template <typename T> int adv_fields(Ctx &c);
 // quasi/quasi.cpp:1099-2190 (nloop = 1-based step counter)

@@ -117,6 +117,8 @@ SIGNATURES = [
     ("smadft_batch_member", ctypes.c_int, [_vp, ctypes.c_int, _P(_vp)]),
     ("smadft_batch_step", ctypes.c_int, [_vp, ctypes.c_int]),
     ("smadft_batch_sync", ctypes.c_int, [_vp]),
+    ("smadft_batch_get_stream", ctypes.c_int, [_vp, _P(_vp)]),
+    ("smadft_batch_groups", ctypes.c_int, [_vp, _P(ctypes.c_int)]),
     ("smadft_batch_last_error", ctypes.c_char_p, [_vp]),
     ("smadft_autotune", ctypes.c_int, [_vp, ctypes.c_int, _P(TuneReport)]),
     ("smadft_adjoint", ctypes.c_int, [_vp, _P(AdjOpts), _P(Grads), _dp]),
@@ -370,6 +372,20 @@ class Batch:
 
     def sync(self) -> None:
         _check(lib().smadft_batch_sync(self._h))
+
+    @property
+    def stream(self) -> int:
+        """The batch's cudaStream_t (every batch step is ordered on it)."""
+        s = _vp()
+        _check(lib().smadft_batch_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    @property
+    def groups(self) -> int:
+        """Number of member groups stepped with pooled fields."""
+        g = ctypes.c_int()
+        _check(lib().smadft_batch_groups(self._h, ctypes.byref(g)))
+        return g.value
 
     def close(self):
         h = getattr(self, "_h", None)

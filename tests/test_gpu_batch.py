@@ -119,3 +119,62 @@ def test_autotune_times_the_gemm_form_z_pass_for_fp32():
             s.step(2)
             assert np.all(np.isfinite(s.get("psi")))
         assert (gemm in rep["ms_per_step"]) == timed, (prec, shape, rep)
+
+
+def test_batch_groups_match_solo_runs():
+    """Members with the same model (noadv / adv), grid and precision form groups whose plain
+    axis passes run as one launch over pooled fields; with different parameters per member
+    (eps, gamma) each still follows its solo run (FP64 to 1e-12, FP32 to 1e-5 relative: the
+    grouped x passes are other instantiations of the same kernels), also interleaved with a
+    member stepped alone, and with grouping off the batch reproduces the solo runs exactly."""
+    cases = [smadft.params(smadft.ADV, (16, 64, 64), precision=smadft.FP32, dt=0.01, eps=-0.7 - 0.05 * i,
+                           gamma=1.0 + 0.1 * i) for i in range(3)]
+    cases += [smadft.params(smadft.NOADV, (32, 24, 40), eps=-0.75 + 0.03 * i) for i in range(3)]
+    cases += [smadft.params(smadft.ADV, (8, 96, 96), precision=smadft.FP32, dt=0.01, eps=-0.7 - 0.1 * i)
+              for i in range(2)]
+    cases += [smadft.params(smadft.QUASI, (24, 20, 32), dt=0.002, kp=0.3, divv_switch=3)]
+    steps = 6
+    solo = []
+    for i, p in enumerate(cases):
+        with smadft.Solver(p) as s:
+            s.set_psi(ic(p, 20 + i))
+            s.step(2)
+            if i == 1:
+                s.step(1)
+            s.step(steps - 2)
+            solo.append((s.get("psi"), s.get("vx") if p.model != smadft.NOADV else None))
+    with smadft.Batch(cases) as b:
+        assert b.groups == 3
+        for i, p in enumerate(cases):
+            b.members[i].set_psi(ic(p, 20 + i))
+        b.step(2)
+        b.members[1].step(1)                 # a grouped member alone, on its pooled fields
+        b.step(steps - 2)
+        b.sync()
+        for i, p in enumerate(cases):
+            tol = 1e-12 if p.precision == smadft.FP64 else 1e-5
+            got, want = b.members[i].get("psi"), solo[i][0]
+            assert np.max(np.abs(got - want)) <= tol * np.max(np.abs(want)), i
+            if solo[i][1] is not None:
+                gv, wv = b.members[i].get("vx"), solo[i][1]
+                assert np.max(np.abs(gv - wv)) <= 10 * tol * np.max(np.abs(wv)), i
+
+
+def test_batch_without_groups_is_exact(monkeypatch):
+    monkeypatch.setenv("SMADFT_BATCH_GROUP", "0")
+    cases = [smadft.params(smadft.ADV, (16, 64, 64), precision=smadft.FP32, dt=0.01, eps=-0.7 - 0.05 * i)
+             for i in range(2)]
+    solo = []
+    for i, p in enumerate(cases):
+        with smadft.Solver(p) as s:
+            s.set_psi(ic(p, 30 + i))
+            s.step(4)
+            solo.append(s.get("psi"))
+    with smadft.Batch(cases) as b:
+        assert b.groups == 0
+        for i, p in enumerate(cases):
+            b.members[i].set_psi(ic(p, 30 + i))
+        b.step(4)
+        b.sync()
+        for i in range(2):
+            assert np.array_equal(b.members[i].get("psi"), solo[i]), i
