@@ -45,7 +45,7 @@ ERR_STEPS = 10000   # steps after which the FP32 psi is compared with the FP64 p
 F_ADV = 32          # compulsory full-field transfers per adv step (single-sweep stages)
 # the kernel the roofline object describes, its key in pass_kernels and its ncu summary
 DOMINANT_PASS = "z_dct3"
-DOMINANT_PROFILE = "r2r_rdz_z_pass_256cube_fp32.md"
+DOMINANT_PROFILE = "r2r_rdz_z_pass_dct3_256cube_fp32.md"
 DOMINANT_KERNEL = ("r2r_rdz_kernel<float,256,DCT-III> plain inverse pass along z (the largest share of the adv "
                    "step's device time); algorithmic bytes per launch = 2 x 4 B x 256^3, 6-field ring")
 

@@ -201,6 +201,13 @@ int smadft_get_stream(smadft_ctx *ctx, void **stream);
 /* Number of kernels this context has launched since creation. */
 int smadft_launch_count(const smadft_ctx *ctx, long long *count);
 
+/* Bounds-check build (`make -C sma-dft_b200 check` -> libsmadft_check.so, compiled with
+ * SMADFT_CHECK_BOUNDS): every element index the axis-pass kernels hand to their loaders and
+ * storers is checked against the field size, and an index outside it sets a device word
+ * instead of touching memory.  *bad = 1 if that happened since the context was created
+ * (synchronises).  The normal library returns SMADFT_ERR_UNSUPPORTED. */
+int smadft_bounds_status(smadft_ctx *ctx, int *bad);
+
 /* One axis pass of a 3-D r2r transform on device buffers (axis 0=x, 1=y, 2=z; kind as
  * below); in may equal out; both 16-byte aligned.  Exposed for tuning and for per-kernel roofline timing. */
 int smadft_r2r_pass_device(smadft_ctx *ctx, const void *in, void *out, int axis, int kind);

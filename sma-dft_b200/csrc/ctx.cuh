@@ -121,6 +121,7 @@ struct Ctx {
     bool use_tma = false;          // FP32 plain strided passes fed by TMA, persistent (SMADFT_TMA_PASS=1)
     int grid_y = 1;                // strided and generic passes: CTA rows (fields of a batch group, LoadArrM)
     bool pooled = false;           // field slots live in a batch group's pools (the batch frees them)
+    int *chk = nullptr;            // bounds-check build: device word set by an out-of-range index
     static constexpr int kMaxFork = 5;
     cudaStream_t aux[kMaxFork] = {};   // forked streams (graph branches under capture)
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxFork] = {};     // fused z + y passes (r2r_plane_kernel) where ny = nz allows
@@ -702,6 +703,9 @@ int pooled_pass(Ctx &lead, int M, int kind, const S *in, T *out)
             return launch_axis<T, 0>(pc, kind, LoadArrM<T, S>{in, (idx_t)lead.n}, StoreArrM<T>{out, (idx_t)lead.n});
         } else {
             pc.g.nx = lead.g.nx * M;
+#ifdef SMADFT_CHECK_BOUNDS
+            pc.g.nelem = lead.g.nelem * M;
+#endif
             return launch_axis<T, AXIS>(pc, kind, LoadArr<T, S>{in}, StoreArr<T>{out});
         }
     });

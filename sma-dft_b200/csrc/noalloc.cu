@@ -238,6 +238,9 @@ extern "C" int smadft_r2r3d_noalloc(const void *in, void *out, int nx, int ny, i
     Geom g;
     g.nx = nx; g.ny = ny; g.nz = nz;
     g.nyz = (long long)ny * nz;
+#ifdef SMADFT_CHECK_BOUNDS
+    g.nelem = (long long)nx * ny * nz;
+#endif
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (precision == SMADFT_FP64)
         return na_transform<double>(g, static_cast<const double *>(in), static_cast<double *>(out), kx, ky, kz, st, *d, dev);

@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(CFG::THREADS, CFG::MINB) r2r_fast_kernel(Geom 
             ww[b] = w;
             const ElemPos p = tile_elem<AXIS>(g, tb, t, w);
             if (vec_ok && (AXIS == 2 || p.k + V <= g.nz)) {
-                if (p.valid) ld.template load<V>(p.idx, p.i, p.j, p.k, vals[b]);
+                if (p.valid && idx_ok(g, p.idx, V)) ld.template load<V>(p.idx, p.i, p.j, p.k, vals[b]);
                 else {
 #pragma unroll
                     for (int u = 0; u < V; u++) vals[b][u] = T(0);
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(CFG::THREADS, CFG::MINB) r2r_fast_kernel(Geom 
             } else {
 #pragma unroll
                 for (int u = 0; u < V; u++) {
-                    if (p.k + u < g.nz) ld.template load<1>(p.idx + u, p.i, p.j, p.k + u, &vals[b][u]);
+                    if (p.k + u < g.nz && idx_ok(g, p.idx + u)) ld.template load<1>(p.idx + u, p.i, p.j, p.k + u, &vals[b][u]);
                     else vals[b][u] = T(0);
                 }
             }
@@ -447,11 +447,11 @@ __global__ void __launch_bounds__(CFG::THREADS, CFG::MINB) r2r_fast_kernel(Geom 
         }
         if (!p.valid) continue;
         if (vec_ok && (AXIS == 2 || p.k + V <= g.nz)) {
-            st.template store<V>(p.idx, p.i, p.j, p.k, v);
+            if (idx_ok(g, p.idx, V)) st.template store<V>(p.idx, p.i, p.j, p.k, v);
         } else {
 #pragma unroll
             for (int u = 0; u < V; u++)
-                if (p.k + u < g.nz) st.template store<1>(p.idx + u, p.i, p.j, p.k + u, &v[u]);
+                if (p.k + u < g.nz && idx_ok(g, p.idx + u)) st.template store<1>(p.idx + u, p.i, p.j, p.k + u, &v[u]);
         }
     }
 }

@@ -23,7 +23,26 @@ using idx_t = int;
 struct Geom {
     int nx, ny, nz;
     int nyz;         // ny * nz
+#ifdef SMADFT_CHECK_BOUNDS
+    long long nelem = 0;   // valid element indices [0, nelem) of the pass's fields
+    int *chk = nullptr;    // device word set to 1 by the first out-of-range index
+#endif
 };
+
+// Bounds-check build (-DSMADFT_CHECK_BOUNDS, `make check`): every element index a pass kernel
+// hands to its loader or storer is checked against the field size; an index outside it sets
+// the context's check word and the access is skipped (loads give zero), so a wrong index
+// shows up as a status instead of a memory fault.  In the normal build the check is `true`.
+#ifdef SMADFT_CHECK_BOUNDS
+__device__ __forceinline__ bool idx_ok(const Geom &g, long long q, int span = 1)
+{
+    if (q >= 0 && q + span <= g.nelem) return true;
+    if (g.chk) atomicCAS(g.chk, 0, 1);
+    return false;
+}
+#else
+__device__ __forceinline__ constexpr bool idx_ok(const Geom &, long long, int = 1) { return true; }
+#endif
 
 template <typename T>
 struct PassArgs {
@@ -356,7 +375,7 @@ __global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST 
         else { w = e % W; t = e / W; }
         ElemPos p = elem_pos(a, t, w);
         T v = T(0);
-        if (p.valid) ld.template load<1>(p.idx, p.i, p.j, p.k, &v);
+        if (p.valid && idx_ok(a.g, p.idx)) ld.template load<1>(p.idx, p.i, p.j, p.k, &v);
         int pos;
         if (kind == K_DCT2) pos = makhoul_pos(t, n);
         else if (kind == K_DST2) { pos = makhoul_pos(t, n); if (t & 1) v = -v; }
@@ -410,7 +429,7 @@ __global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST 
             v = (w & 1) ? z.y : z.x;
             if (kind == K_DST3 && (o & 1)) v = -v;
         }
-        if (p.valid) st.template store<1>(p.idx, p.i, p.j, p.k, &v);
+        if (p.valid && idx_ok(a.g, p.idx)) st.template store<1>(p.idx, p.i, p.j, p.k, &v);
     }
 }
 

@@ -391,8 +391,12 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()
         const int t = pos.src(q);
         const int ii = AXIS == 1 ? a : t, jj = AXIS == 1 ? t : a;
         T v[2] = {T(0), T(0)};
-        if (!edge || nk >= 2) l.template load<2>(src_idx(q), ii, jj, k, v);
-        else if (nk == 1) l.template load<1>(src_idx(q), ii, jj, k, v);
+        const idx_t si = src_idx(q);
+        if (!edge || nk >= 2) {
+            if (idx_ok(g, si, 2)) l.template load<2>(si, ii, jj, k, v);
+        } else if (nk == 1) {
+            if (idx_ok(g, si)) l.template load<1>(si, ii, jj, k, v);
+        }
         return {v[0], v[1]};
     };
 
@@ -430,8 +434,11 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()
         const idx_t q = out_idx(pnt);
         const int ii = AXIS == 1 ? a : o, jj = AXIS == 1 ? o : a;
         const T w2[2] = {z.x, z.y};
-        if (!edge || nk >= 2) fin_c<2>(st, comp, q, ii, jj, k, w2, pre_buf);
-        else if (nk == 1) store_c<1>(st, comp, q, ii, jj, k, w2);
+        if (!edge || nk >= 2) {
+            if (idx_ok(g, q, 2)) fin_c<2>(st, comp, q, ii, jj, k, w2, pre_buf);
+        } else if (nk == 1) {
+            if (idx_ok(g, q)) store_c<1>(st, comp, q, ii, jj, k, w2);
+        }
     };
     if (full) {
 #pragma unroll
@@ -440,7 +447,8 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()
 #pragma unroll
             for (int u = 0; u < CH; u++) {
                 const int o = out_row(p0 + u);
-                pre_c<2>(st, comp, out_idx(p0 + u), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
+                if (idx_ok(g, out_idx(p0 + u), 2))
+                    pre_c<2>(st, comp, out_idx(p0 + u), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
             }
 #pragma unroll
             for (int u = 0; u < CH; u++) put(p0 + u, false, pre_buf[u]);
@@ -450,7 +458,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, rd_min_blocks<T, LD, ST>()
         for (int p0 = 0; p0 < NP; p0++) {
             PB pre_buf[PL];
             const int o = out_row(p0);
-            if (nk >= 2) pre_c<2>(st, comp, out_idx(p0), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
+            if (nk >= 2 && idx_ok(g, out_idx(p0), 2)) pre_c<2>(st, comp, out_idx(p0), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
             put(p0, true, pre_buf);
         }
     }

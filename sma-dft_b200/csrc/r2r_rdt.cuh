@@ -178,8 +178,11 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2)
             const idx_t q = out_idx(pnt);
             const int ii = AXIS == 1 ? a : o, jj = AXIS == 1 ? o : a;
             const T w2[2] = {z.x, z.y};
-            if (!edge || nk >= 2) fin_c<2>(st, 0, q, ii, jj, k, w2, pre_buf);
-            else if (nk == 1) store_c<1>(st, 0, q, ii, jj, k, w2);
+            if (!edge || nk >= 2) {
+                if (idx_ok(g, q, 2)) fin_c<2>(st, 0, q, ii, jj, k, w2, pre_buf);
+            } else if (nk == 1) {
+                if (idx_ok(g, q)) store_c<1>(st, 0, q, ii, jj, k, w2);
+            }
         };
         if (full) {
 #pragma unroll
@@ -188,6 +191,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2)
 #pragma unroll
                 for (int u = 0; u < CH; u++) {
                     const int o = pos.out(p0 + u);
+                    if (idx_ok(g, out_idx(p0 + u), 2))
                     pre_c<2>(st, 0, out_idx(p0 + u), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf[u]);
                 }
 #pragma unroll
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, 2)
             for (int p0 = 0; p0 < NP; p0++) {
                 PB pre_buf[PL];
                 const int o = pos.out(p0);
-                if (nk >= 2) pre_c<2>(st, 0, out_idx(p0), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
+                if (nk >= 2 && idx_ok(g, out_idx(p0), 2)) pre_c<2>(st, 0, out_idx(p0), AXIS == 1 ? a : o, AXIS == 1 ? o : a, k, pre_buf);
                 put(p0, true, pre_buf);
             }
         }

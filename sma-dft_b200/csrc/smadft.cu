@@ -537,6 +537,12 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
         cudaGetLastError();
         c.num_sms = 148;
     }
+#ifdef SMADFT_CHECK_BOUNDS
+    if (cudaMalloc(&c.chk, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
+    if (cudaMemset(c.chk, 0, sizeof(int)) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
+    c.g.nelem = c.n;
+    c.g.chk = c.chk;
+#endif
     if (c.f32) {   // error word of the GEMM-form passes
         if (cudaMalloc(&c.gz_err, sizeof(int)) != cudaSuccess) { cudaGetLastError(); return bail(SMADFT_ERR_NOMEM); }
         if (cudaMemset(c.gz_err, 0, sizeof(int)) != cudaSuccess) return bail(SMADFT_ERR_CUDA);
@@ -561,6 +567,7 @@ int smadft_destroy(smadft_ctx *h)
         if (kv.second.gz) cudaFree(kv.second.gz);
     }
     if (c.gz_err) cudaFree(c.gz_err);
+    if (c.chk) cudaFree(c.chk);
     if (c.tables64 && c.tables64 != c.tables) cudaFree(c.tables64);
     if (c.tables) cudaFree(c.tables);
     if (c.red) cudaFree(c.red);
@@ -836,6 +843,21 @@ int smadft_launch_count(const smadft_ctx *h, long long *count)
     if (!h || !count) return SMADFT_ERR_INVALID;
     *count = h->c.launches;
     return SMADFT_OK;
+}
+
+int smadft_bounds_status(smadft_ctx *h, int *bad)
+{
+    if (!h || !bad) return SMADFT_ERR_INVALID;
+    *bad = 0;
+#ifdef SMADFT_CHECK_BOUNDS
+    Ctx &c = h->c;
+    cudaSetDevice(c.dev);
+    SMADFT_CUDA(cudaStreamSynchronize(c.stream));
+    SMADFT_CUDA(cudaMemcpy(bad, c.chk, sizeof(int), cudaMemcpyDeviceToHost));
+    return SMADFT_OK;
+#else
+    return SMADFT_ERR_UNSUPPORTED;
+#endif
 }
 
 int smadft_r2r_pass_device(smadft_ctx *h, const void *in, void *out, int axis, int kind)

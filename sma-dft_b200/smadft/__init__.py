@@ -14,7 +14,9 @@ import subprocess
 import numpy as np
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libsmadft.so")
+# SMADFT_LIB selects another build of the library in this directory (libsmadft_check.so: the
+# bounds-check build)
+LIB_PATH = os.path.join(PKG_DIR, os.environ.get("SMADFT_LIB", "libsmadft.so"))
 
 NOADV, ADV, QUASI, COMP = 0, 1, 2, 3
 FP64, FP32 = 0, 1
@@ -117,6 +119,7 @@ SIGNATURES = [
     ("smadft_batch_member", ctypes.c_int, [_vp, ctypes.c_int, _P(_vp)]),
     ("smadft_batch_step", ctypes.c_int, [_vp, ctypes.c_int]),
     ("smadft_batch_sync", ctypes.c_int, [_vp]),
+    ("smadft_bounds_status", ctypes.c_int, [_vp, _P(ctypes.c_int)]),
     ("smadft_batch_get_stream", ctypes.c_int, [_vp, _P(_vp)]),
     ("smadft_batch_groups", ctypes.c_int, [_vp, _P(ctypes.c_int)]),
     ("smadft_batch_last_error", ctypes.c_char_p, [_vp]),
@@ -195,6 +198,14 @@ def ic_conics(p: Params, A=0.5, count=4, rmin=3.0, rmax=6.0, noise=1e-3, seed=20
     out = np.empty((p.nx, p.ny, p.nz), dtype=np.float64)
     _check(lib().smadft_ic_conics(ctypes.byref(p), A, count, rmin, rmax, noise, seed, _dptr(out)))
     return out
+
+
+def bounds_status(solver) -> int:
+    """1 if the bounds-check build saw an out-of-range index in this context, 0 if not; the
+    normal build returns SMADFT_ERR_UNSUPPORTED (-6)."""
+    bad = ctypes.c_int()
+    rc = lib().smadft_bounds_status(solver._h, ctypes.byref(bad))
+    return rc if rc else bad.value
 
 
 def r2r3d_noalloc(src_ptr: int, dst_ptr: int, shape, kinds, precision: int = FP64, stream: int = 0) -> int:
