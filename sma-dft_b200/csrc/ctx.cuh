@@ -119,6 +119,7 @@ struct Ctx {
     int num_sms = 148;             // persistent grids (GEMM-form passes): one CTA per SM
     int *gz_err = nullptr;         // device word: nonzero when a GEMM-form pass gave up a bounded wait
     bool use_tma = false;          // FP32 plain strided passes fed by TMA, persistent (SMADFT_TMA_PASS=1)
+    bool share_grad = true;        // adv: gradients reuse psi's y and z passes (SMADFT_SHARE_GRAD=0: not)
     int grid_y = 1;                // strided and generic passes: CTA rows (fields of a batch group, LoadArrM)
     bool pooled = false;           // field slots live in a batch group's pools (the batch frees them)
     int *chk = nullptr;            // bounds-check build: device word set by an out-of-range index
@@ -312,9 +313,10 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
     return SMADFT_OK;
 }
 
-// plain z pass of length N through the register-direct z kernel (in == out allowed)
-template <typename T, int N, int KIND, bool STAGE = false>
-int launch_rdz_k(Ctx &c, int kind, const T *in, T *out)
+// plain z pass of length N through the register-direct z kernel (in == out allowed); with
+// zs, the pass of the shifted gradient spectrum along z (in != out)
+template <typename T, int N, int KIND, bool STAGE = false, bool GRADZ = false>
+int launch_rdz_k(Ctx &c, int kind, const T *in, T *out, const T *zs = nullptr)
 {
     const PlanDev &pd = c.plans.at(N);
     const int rows = c.g.nx * c.g.ny;
@@ -324,14 +326,14 @@ int launch_rdz_k(Ctx &c, int kind, const T *in, T *out)
     {
         std::lock_guard<std::mutex> lock(attr_mutex());
         if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N, KIND, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem));
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N, KIND, STAGE, GRADZ>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_rdz_kernel<T, N, KIND, STAGE><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+    r2r_rdz_kernel<T, N, KIND, STAGE, GRADZ><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h),
-        c.rdz_rev ? 1 : 0);
+        c.rdz_rev ? 1 : 0, zs);
     SMADFT_CUDA(cudaGetLastError());
     c.launches++;
     return SMADFT_OK;
@@ -345,13 +347,24 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
     // inverse kinds stage their outputs through shared memory when `out` allows 16-byte stores
     const bool stage = c.rdz_stage && ((uintptr_t)out & 15) == 0;
     switch (kind) {
-    case K_DCT2: return launch_rdz_k<T, N, K_DCT2>(c, kind, in, out);
+    case K_DCT2: return launch_rdz_k<T, N, K_DCT2, false>(c, kind, in, out);
     case K_DCT3:
-        return stage ? launch_rdz_k<T, N, K_DCT3, true>(c, kind, in, out) : launch_rdz_k<T, N, K_DCT3>(c, kind, in, out);
-    case K_DST2: return launch_rdz_k<T, N, K_DST2>(c, kind, in, out);
+        return stage ? launch_rdz_k<T, N, K_DCT3, true>(c, kind, in, out)
+                     : launch_rdz_k<T, N, K_DCT3, false>(c, kind, in, out);
+    case K_DST2: return launch_rdz_k<T, N, K_DST2, false>(c, kind, in, out);
     default:
-        return stage ? launch_rdz_k<T, N, K_DST3, true>(c, kind, in, out) : launch_rdz_k<T, N, K_DST3>(c, kind, in, out);
+        return stage ? launch_rdz_k<T, N, K_DST3, true>(c, kind, in, out)
+                     : launch_rdz_k<T, N, K_DST3, false>(c, kind, in, out);
     }
+}
+
+// z pass of the shifted gradient spectrum along z (LdGrad<T, 2, T>), inverse sine kind: the
+// gradient's z transform in the psi / grad psi family
+template <typename T, int N>
+int launch_rdz_gradz(Ctx &c, const T *in, T *out, const T *zs)
+{
+    if (((uintptr_t)out & 15) == 0 && c.rdz_stage) return launch_rdz_k<T, N, K_DST3, true, true>(c, K_DST3, in, out, zs);
+    return launch_rdz_k<T, N, K_DST3, false, true>(c, K_DST3, in, out, zs);
 }
 
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link

@@ -78,6 +78,23 @@ struct LdGrad {
     }
 };
 
+// Inverse sine z pass of the shifted gradient spectrum of f along z (LdGrad<T, 2, T>) into out
+// (out != f): the register-direct z kernel reads the shifted, scaled line itself where the
+// length has it, else the loader runs in the staged z pass.
+template <typename T>
+int z_pass_grad(Ctx &c, const Spec<T> &s, const T *f, T *out)
+{
+    if (c.use_rd && c.use_rdz && f != out) {
+        switch (c.g.nz) {
+        case 64: return launch_rdz_gradz<T, 64>(c, f, out, s.sz);
+        case 128: return launch_rdz_gradz<T, 128>(c, f, out, s.sz);
+        case 256: return launch_rdz_gradz<T, 256>(c, f, out, s.sz);
+        default: break;
+        }
+    }
+    return launch_axis<T, 2>(c, K_DST3, LdGrad<T, 2, T>{s, f}, StoreArr<T>{out});
+}
+
 // -L(q) psihat (adv/cosAdvTrackMult.cpp:980-986)
 template <typename T>
 struct LdNegLin {

@@ -31,10 +31,13 @@ constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * s
 // STAGE: the outputs go through shared memory and leave as whole rows in 16-byte stores (the
 // inverse kinds' Makhoul order would otherwise scatter every warp store over every second
 // element); `out` must then be 16-byte aligned.
-template <typename T, int N, int KIND = -1, bool STAGE = false>
+// GRADZ: the line read is the index-shifted gradient spectrum of `in` along z (LdGrad along
+// z): point n takes -zs[n] in[n + 1], and the last point 0; `out` must then differ from `in`.
+template <typename T, int N, int KIND = -1, bool STAGE = false, bool GRADZ = false>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind_rt, const T *in, T *out,
                                                                         const cpx<T> *__restrict__ wt_g,
-                                                                        const cpx<T> *__restrict__ ht_g, int rev)
+                                                                        const cpx<T> *__restrict__ ht_g, int rev,
+                                                                        const T *__restrict__ zs)
 {
     const int kind = KIND >= 0 ? KIND : kind_rt;
     using RI = RdInfo<N>;
@@ -66,7 +69,17 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
 #pragma unroll
     for (int q = 0; q < R0; q++) {
         const int n = pos.src(q);
-        T a = pa[n], b = pb[n];
+        T a, b;
+        if constexpr (GRADZ) {
+            const bool inr = n < N - 1;
+            const int m = inr ? n + 1 : n;
+            const T sc = inr ? -zs[n] : T(0);
+            a = sc * pa[m];
+            b = sc * pb[m];
+        } else {
+            a = pa[n];
+            b = pb[n];
+        }
         if (!oka) a = T(0);
         if (!okb) b = T(0);
         if (fwd && sine && !RdPos<N>::src_lo(q)) {   // DST-II negates odd natural samples
@@ -83,12 +96,29 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
         // of N elements out with 16-byte stores; rows past `rows` are not written
         T *sb = reinterpret_cast<T *>(buf);
         __syncthreads();                                 // every warp is done with buf
+        if constexpr (R1 == 16 && BPT == 1) {
+            // the two half-warps of a warp write rows 2N apart (same banks) and each point
+            // goes to every second element; the odd line takes its points half a turn later,
+            // so in each store one half-warp writes even and the other odd elements
+            const bool odd = c & 1;
 #pragma unroll
-        for (int pnt = 0; pnt < NP; pnt++) {
-            const cpx<T> z = x1[pnt / R1][pnt % R1];
-            const int o = pos.out(pnt);
-            sb[(2 * c) * N + o] = z.x;
-            sb[(2 * c + 1) * N + o] = z.y;
+            for (int pnt = 0; pnt < NP; pnt++) {
+                constexpr int H = NP / 2;
+                const int pt = (pnt + H) % NP;
+                const cpx<T> z0 = x1[0][pnt], z1 = x1[0][pt];
+                const int o = odd ? pos.out(pt) : pos.out(pnt);
+                const T zx = odd ? z1.x : z0.x, zy = odd ? z1.y : z0.y;
+                sb[(2 * c) * N + o] = zx;
+                sb[(2 * c + 1) * N + o] = zy;
+            }
+        } else {
+#pragma unroll
+            for (int pnt = 0; pnt < NP; pnt++) {
+                const cpx<T> z = x1[pnt / R1][pnt % R1];
+                const int o = pos.out(pnt);
+                sb[(2 * c) * N + o] = z.x;
+                sb[(2 * c + 1) * N + o] = z.y;
+            }
         }
         __syncthreads();
         constexpr int VEC = 16 / (int)sizeof(T);

@@ -4,6 +4,39 @@
 
 namespace smadft {
 
+// psi, grad psi and Sp2 = iCT(-L psihat) from psihat with the passes the gradients share with
+// psi.  The gradient spectra are index-shifted, scaled copies of psihat along one axis
+// (LdGrad), and shifting or scaling along one axis commutes with the transforms along the
+// others.  So psi's y pass output P = iCT_y(psihat) also gives gz = iCT_x iST_z (LdGrad_z P),
+// and psi's y + z output U = iCT_z P gives gx = iST_x (LdGrad_x U): the y passes of gx and gz
+// and the z pass of gx are not run (12 axis passes instead of 15).  The order of operations
+// differs from the reference's (scale, then transform) only in rounding.
+template <typename T>
+int adv_psi_fields_shared(Ctx &c, const Spec<T> &s, const double *ph, T *psi, T *gx, T *gy, T *gz, T *sp2)
+{
+    const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
+    T *const out[3] = {psi, gy, sp2};
+    int rc = y_pass_multi<T, 3, 0>(c, ky, out, LoadArr<T, double>{ph}, LdGrad<T, 1, double>{s, ph}, LdNegLin<T>{s, ph});
+    if (rc) return rc;
+    // gz's z pass reads P before psi's z pass replaces it
+    if ((rc = z_pass_grad<T>(c, s, psi, gz))) return rc;
+    return forked(c, 4, [&](int m) {
+        int r;
+        switch (m) {
+        case 0:   // psi: z pass, then gx's x pass reads U before psi's x pass replaces it
+            if ((r = launch_axis<T, 2>(c, K_DCT3, LoadArr<T>{psi}, StoreArr<T>{psi}))) return r;
+            if ((r = launch_axis<T, 0>(c, K_DST3, LdGrad<T, 0, T>{s, psi}, StoreArr<T>{gx}))) return r;
+            return launch_axis<T, 0>(c, K_DCT3, LoadArr<T>{psi}, StoreArr<T>{psi});
+        case 1: return launch_axis<T, 0>(c, K_DCT3, LoadArr<T>{gz}, StoreArr<T>{gz});
+        default: {
+            T *f = m == 2 ? gy : sp2;
+            if ((r = launch_axis<T, 2>(c, K_DCT3, LoadArr<T>{f}, StoreArr<T>{f}))) return r;
+            return launch_axis<T, 0>(c, K_DCT3, LoadArr<T>{f}, StoreArr<T>{f});
+        }
+        }
+    });
+}
+
 // psi, grad psi, Sp2, the force spectra S-hat and the velocity v of the current psihat: the
 // loop body up to N (adv/cosAdvTrackMult.cpp:847-1286)
 template <typename T>
@@ -17,7 +50,9 @@ int adv_fields(Ctx &c)
     T *vx = c.f<T>(S_VX), *vy = c.f<T>(S_VY), *vz = c.f<T>(S_VZ);
     int rc;
     // psi, grad psi and Sp2 = iCT(-L psihat), all from psihat (adv/cosAdvTrackMult.cpp:904-991)
-    {
+    if (c.share_grad && c.use_rd && c.use_multi && !plane_ok(c) && (c.g.ny == 64 || c.g.ny == 128 || c.g.ny == 256)) {
+        if ((rc = adv_psi_fields_shared<T>(c, s, ph, psi, gx, gy, gz, sp2))) return rc;
+    } else {
         const int kx[5] = {K_DCT3, K_DST3, K_DCT3, K_DCT3, K_DCT3};
         const int ky[5] = {K_DCT3, K_DCT3, K_DST3, K_DCT3, K_DCT3};
         const int kz[5] = {K_DCT3, K_DCT3, K_DCT3, K_DST3, K_DCT3};
@@ -89,7 +124,33 @@ int adv_group_step(Ctx *const *mm, int M)
     auto pz = [&](int slot, int kind) { return pooled_pass<T, 2>(L, M, kind, L.f<T>(slot), L.f<T>(slot)); };
     auto px = [&](int slot, int kind) { return pooled_pass<T, 0>(L, M, kind, L.f<T>(slot), L.f<T>(slot)); };
     // psi, grad psi and Sp2 from psihat (adv/cosAdvTrackMult.cpp:904-991)
-    {
+    if (L.share_grad && L.use_rd && L.use_multi && (L.g.ny == 64 || L.g.ny == 128 || L.g.ny == 256)) {
+        // the shared-pass order of adv_psi_fields_shared: the passes that carry a member's
+        // wavenumbers (gz's z pass, gx's x pass) run per member, the plain ones over the pool
+        const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                Spec<T> s = make_spec<T>(c);
+                double *ph = c.f<double>(S_PSIH);
+                T *const out[3] = {c.f<T>(S_PSI), c.f<T>(S_GY), c.f<T>(S_SP2)};
+                const int r = y_pass_multi<T, 3, 0>(c, ky, out, LoadArr<T, double>{ph}, LdGrad<T, 1, double>{s, ph},
+                                                    LdNegLin<T>{s, ph});
+                return r ? r : z_pass_grad<T>(c, s, c.f<T>(S_PSI), c.f<T>(S_GZ));
+            });
+            if (rc) return rc;
+        }
+        if ((rc = pz(S_PSI, K_DCT3))) return rc;
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                return launch_axis<T, 0>(c, K_DST3, LdGrad<T, 0, T>{make_spec<T>(c), c.f<T>(S_PSI)},
+                                         StoreArr<T>{c.f<T>(S_GX)});
+            });
+            if (rc) return rc;
+        }
+        if ((rc = px(S_PSI, K_DCT3)) || (rc = px(S_GZ, K_DCT3))) return rc;
+        for (int slot : {S_GY, S_SP2})
+            if ((rc = pz(slot, K_DCT3)) || (rc = px(slot, K_DCT3))) return rc;
+    } else {
         const int kx[5] = {K_DCT3, K_DST3, K_DCT3, K_DCT3, K_DCT3};
         const int ky[5] = {K_DCT3, K_DCT3, K_DST3, K_DCT3, K_DCT3};
         const int kz[5] = {K_DCT3, K_DCT3, K_DCT3, K_DST3, K_DCT3};
