@@ -60,56 +60,132 @@ __device__ __forceinline__ cpx<T> tw(const cpx<T> *__restrict__ w, int e)
     return t;
 }
 
+// ---- complex arithmetic on the packed (real, imaginary) pair -----------------------------
+// FP32 sums, differences and real-scalar multiply-adds of a pair run as one packed two-lane
+// instruction (sm_100: add / sub / mul / fma .rn.f32x2), which rounds each lane exactly as the
+// scalar instruction would; FP64 stays scalar.
+template <typename T>
+__device__ __forceinline__ cpx<T> mul_mi(cpx<T> a) { return {a.y, -a.x}; }   // -i a
+template <typename T>
+__device__ __forceinline__ cpx<T> mul_pi(cpx<T> a) { return {-a.y, a.x}; }   // +i a
+template <typename T>
+__device__ __forceinline__ cpx<T> cadd(cpx<T> a, cpx<T> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename T>
+__device__ __forceinline__ cpx<T> csub(cpx<T> a, cpx<T> b) { return {a.x - b.x, a.y - b.y}; }
+// a + s b, s real (one rounding per lane)
+template <typename T>
+__device__ __forceinline__ cpx<T> caxpy(cpx<T> a, T s, cpx<T> b) { return {fma(s, b.x, a.x), fma(s, b.y, a.y)}; }
+// s b, s real
+template <typename T>
+__device__ __forceinline__ cpx<T> cscale(T s, cpx<T> b) { return {s * b.x, s * b.y}; }
+
+__device__ __forceinline__ unsigned long long pk2(cpx<float> a)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ cpx<float> upk2(unsigned long long r)
+{
+    cpx<float> a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+template <>
+__device__ __forceinline__ cpx<float> cadd<float>(cpx<float> a, cpx<float> b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(r);
+}
+template <>
+__device__ __forceinline__ cpx<float> csub<float>(cpx<float> a, cpx<float> b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(r);
+}
+template <>
+__device__ __forceinline__ cpx<float> caxpy<float>(cpx<float> a, float s, cpx<float> b)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(b)), "l"(pk2(cpx<float>{s, s})), "l"(pk2(a)));
+    return upk2(r);
+}
+template <>
+__device__ __forceinline__ cpx<float> cscale<float>(float s, cpx<float> b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(cpx<float>{s, s})), "l"(pk2(b)));
+    return upk2(r);
+}
+
+// DCT-III pre-twiddle of a packed pair of lines (line A in the real parts, line B in the
+// imaginary parts): Z_t = V_A[t] + i V_B[t] with V[t] = exp(+i pi t/2n) (X_t - i X_{n-t}).
+// With xa = X_t and xb = X_{n-t} of both lines and h = exp(+i pi t/2n) this is
+// Z_t = h (xa - i xb): one complex product.
+template <typename T>
+__device__ __forceinline__ cpx<T> dct3_pre(cpx<T> xa, cpx<T> xb, cpx<T> h)
+{
+    return cmul(cpx<T>{xa.x + xb.y, xa.y - xb.x}, h);
+}
+
+// DCT-II post-twiddle of a packed pair of lines: the outputs (line A, line B) at k from
+// Z_k, Z_{n-k} and h = (cos, sin) of pi k/2n, with P = Z_k + Z_{n-k}, D = Z_k - Z_{n-k}:
+//   A_k = h.x P.x + h.y D.y,   B_k = h.x P.y - h.y D.x
+template <typename T>
+__device__ __forceinline__ cpx<T> dct2_post(cpx<T> zk, cpx<T> zm, cpx<T> h)
+{
+    const cpx<T> p = cadd(zk, zm), d = csub(zk, zm);
+    return {fma(h.y, d.y, h.x * p.x), fma(-h.y, d.x, h.x * p.y)};
+}
+
 // Size-R DFT in registers.  Forward uses exp(-2 pi i/R), inverse exp(+2 pi i/R).
 template <int R, typename T, bool INV>
 __device__ __forceinline__ void dft(cpx<T> *v)
 {
     if (R == 2) {
-        cpx<T> a = v[0], b = v[1];
-        v[0] = {a.x + b.x, a.y + b.y};
-        v[1] = {a.x - b.x, a.y - b.y};
+        const cpx<T> a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
     } else if (R == 4) {
-        cpx<T> s0 = {v[0].x + v[2].x, v[0].y + v[2].y};
-        cpx<T> d0 = {v[0].x - v[2].x, v[0].y - v[2].y};
-        cpx<T> s1 = {v[1].x + v[3].x, v[1].y + v[3].y};
-        cpx<T> d1 = {v[1].x - v[3].x, v[1].y - v[3].y};
+        const cpx<T> s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
+        const cpx<T> s1 = cadd(v[1], v[3]), d1 = csub(v[1], v[3]);
         // forward: X1 = d0 - i d1 ; inverse: X1 = d0 + i d1
-        cpx<T> j = INV ? cpx<T>{-d1.y, d1.x} : cpx<T>{d1.y, -d1.x};
-        v[0] = {s0.x + s1.x, s0.y + s1.y};
-        v[2] = {s0.x - s1.x, s0.y - s1.y};
-        v[1] = {d0.x + j.x, d0.y + j.y};
-        v[3] = {d0.x - j.x, d0.y - j.y};
+        const cpx<T> j = INV ? mul_pi(d1) : mul_mi(d1);
+        v[0] = cadd(s0, s1);
+        v[2] = csub(s0, s1);
+        v[1] = cadd(d0, j);
+        v[3] = csub(d0, j);
     } else if (R == 3) {
         const T h = T(0.86602540378443864676372317075294);  // sin(2 pi/3)
-        cpx<T> t1 = {v[1].x + v[2].x, v[1].y + v[2].y};
-        cpx<T> d = {v[1].x - v[2].x, v[1].y - v[2].y};
-        cpx<T> m = {v[0].x - T(0.5) * t1.x, v[0].y - T(0.5) * t1.y};
+        const cpx<T> t1 = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+        const cpx<T> m = caxpy(v[0], T(-0.5), t1);
         // forward: X1 = m - i h d ; X2 = m + i h d
-        cpx<T> q = INV ? cpx<T>{-h * d.y, h * d.x} : cpx<T>{h * d.y, -h * d.x};
-        v[0] = {v[0].x + t1.x, v[0].y + t1.y};
-        v[1] = {m.x + q.x, m.y + q.y};
-        v[2] = {m.x - q.x, m.y - q.y};
+        const cpx<T> hd = cscale(h, d);
+        const cpx<T> q = INV ? mul_pi(hd) : mul_mi(hd);
+        v[0] = cadd(v[0], t1);
+        v[1] = cadd(m, q);
+        v[2] = csub(m, q);
     } else if (R == 5) {
         const T c1 = T(0.30901699437494742410229341718282);   // cos(2 pi/5)
         const T c2 = T(-0.80901699437494742410229341718282);  // cos(4 pi/5)
         const T s1 = T(0.95105651629515357211643933337938);   // sin(2 pi/5)
         const T s2 = T(0.58778525229247312916870595463907);   // sin(4 pi/5)
-        cpx<T> t1 = {v[1].x + v[4].x, v[1].y + v[4].y};
-        cpx<T> t2 = {v[2].x + v[3].x, v[2].y + v[3].y};
-        cpx<T> t3 = {v[1].x - v[4].x, v[1].y - v[4].y};
-        cpx<T> t4 = {v[2].x - v[3].x, v[2].y - v[3].y};
-        cpx<T> a1 = {v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y};
-        cpx<T> a2 = {v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y};
-        cpx<T> b1 = {s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y};
-        cpx<T> b2 = {s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y};
+        const cpx<T> t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        const cpx<T> t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const cpx<T> a1 = caxpy(caxpy(v[0], c1, t1), c2, t2);
+        const cpx<T> a2 = caxpy(caxpy(v[0], c2, t1), c1, t2);
+        const cpx<T> b1 = caxpy(cscale(s1, t3), s2, t4);
+        const cpx<T> b2 = caxpy(cscale(s2, t3), -s1, t4);
         // forward: X1 = a1 - i b1, X4 = a1 + i b1, X2 = a2 - i b2, X3 = a2 + i b2
-        cpx<T> ib1 = INV ? cpx<T>{-b1.y, b1.x} : cpx<T>{b1.y, -b1.x};
-        cpx<T> ib2 = INV ? cpx<T>{-b2.y, b2.x} : cpx<T>{b2.y, -b2.x};
-        v[0] = {v[0].x + t1.x + t2.x, v[0].y + t1.y + t2.y};
-        v[1] = {a1.x + ib1.x, a1.y + ib1.y};
-        v[4] = {a1.x - ib1.x, a1.y - ib1.y};
-        v[2] = {a2.x + ib2.x, a2.y + ib2.y};
-        v[3] = {a2.x - ib2.x, a2.y - ib2.y};
+        const cpx<T> ib1 = INV ? mul_pi(b1) : mul_mi(b1);
+        const cpx<T> ib2 = INV ? mul_pi(b2) : mul_mi(b2);
+        v[0] = cadd(cadd(v[0], t1), t2);
+        v[1] = cadd(a1, ib1);
+        v[4] = csub(a1, ib1);
+        v[2] = cadd(a2, ib2);
+        v[3] = csub(a2, ib2);
     }
 }
 

@@ -66,15 +66,6 @@ struct PlanInfo {
 
 // ---- register codelets -----------------------------------------------------------------
 // Size-R DFT of v[0..R-1] in place, in-order output.  INV selects exp(+2 pi i / R).
-template <typename T>
-__device__ __forceinline__ cpx<T> mul_mi(cpx<T> a) { return {a.y, -a.x}; }   // -i a
-template <typename T>
-__device__ __forceinline__ cpx<T> mul_pi(cpx<T> a) { return {-a.y, a.x}; }   // +i a
-template <typename T>
-__device__ __forceinline__ cpx<T> cadd(cpx<T> a, cpx<T> b) { return {a.x + b.x, a.y + b.y}; }
-template <typename T>
-__device__ __forceinline__ cpx<T> csub(cpx<T> a, cpx<T> b) { return {a.x - b.x, a.y - b.y}; }
-
 template <typename T, bool INV>
 __device__ __forceinline__ void dft4(cpx<T> &a0, cpx<T> &a1, cpx<T> &a2, cpx<T> &a3)
 {
@@ -309,7 +300,8 @@ constexpr size_t fast_smem_bytes() { return ((size_t)(CFG::W / 2) * PlanInfo<N>:
 template <typename T>
 __device__ __forceinline__ T dct2_out(cpx<T> zk, cpx<T> zm, cpx<T> hh, int odd)
 {
-    return odd ? hh.x * (zk.y + zm.y) - hh.y * (zk.x - zm.x) : hh.x * (zk.x + zm.x) + hh.y * (zk.y - zm.y);
+    const cpx<T> o = dct2_post(zk, zm, hh);
+    return odd ? o.y : o.x;
 }
 
 template <typename T, int N, int AXIS, class LD, class ST, class CFG = FastDefault>
@@ -403,20 +395,8 @@ __global__ void __launch_bounds__(CFG::THREADS, CFG::MINB) r2r_fast_kernel(Geom 
             const int tm = N - t;
             cpx<T> xa = L[pa];
             cpx<T> xb = (t == 0) ? cpx<T>{T(0), T(0)} : L[PI::phys(tm)];
-            {
-                const cpx<T> hh = ht[t];
-                const T cc = hh.x, ss = hh.y;
-                T var = cc * xa.x + ss * xb.x, vai = ss * xa.x - cc * xb.x;
-                T vbr = cc * xa.y + ss * xb.y, vbi = ss * xa.y - cc * xb.y;
-                L[pa] = {var - vbi, vai + vbr};
-            }
-            if (t != 0 && tm != t) {
-                const cpx<T> hh = ht[tm];
-                const T cc = hh.x, ss = hh.y;
-                T var = cc * xb.x + ss * xa.x, vai = ss * xb.x - cc * xa.x;
-                T vbr = cc * xb.y + ss * xa.y, vbi = ss * xb.y - cc * xa.y;
-                L[PI::phys(tm)] = {var - vbi, vai + vbr};
-            }
+            L[pa] = dct3_pre(xa, xb, ht[t]);
+            if (t != 0 && tm != t) L[PI::phys(tm)] = dct3_pre(xb, xa, ht[tm]);
         }
         __syncthreads();
         fft_dif<T, N, true>(buf, NL, wt);

@@ -397,12 +397,7 @@ __global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST 
             const cpx<T> *L = bufA + c * a.ld;
             cpx<T> xt = L[t];
             cpx<T> xm = (t == 0) ? cpx<T>{T(0), T(0)} : L[n - t];
-            cpx<T> hh = a.P.h[t];   // (cos, sin) of pi t / 2n
-            T cc = hh.x, ss = hh.y;
-            // V_A = (c A_t + s A_m) + i (s A_t - c A_m), same for B; Z = V_A + i V_B
-            T var = cc * xt.x + ss * xm.x, vai = ss * xt.x - cc * xm.x;
-            T vbr = cc * xt.y + ss * xm.y, vbi = ss * xt.y - cc * xm.y;
-            bufB[c * a.ld + t] = {var - vbi, vai + vbr};
+            bufB[c * a.ld + t] = dct3_pre(xt, xm, a.P.h[t]);
         }
         __syncthreads();
         res = fft_lines<T, true>(bufB, bufA, nl, a.ld, a.P);
@@ -420,10 +415,8 @@ __global__ void __launch_bounds__(256) r2r_pass_kernel(PassArgs<T> a, LD ld, ST 
             const int k = (kind == K_DCT2) ? o : (n - 1 - o);
             cpx<T> zk = L[k];
             cpx<T> zm = L[k == 0 ? 0 : n - k];
-            cpx<T> hh = a.P.h[k];
-            T cc = hh.x, ss = hh.y;
-            if ((w & 1) == 0) v = cc * (zk.x + zm.x) + ss * (zk.y - zm.y);
-            else v = cc * (zk.y + zm.y) - ss * (zk.x - zm.x);
+            const cpx<T> o = dct2_post(zk, zm, a.P.h[k]);
+            v = (w & 1) ? o.y : o.x;
         } else {
             cpx<T> z = L[makhoul_pos(o, n)];
             v = (w & 1) ? z.y : z.x;

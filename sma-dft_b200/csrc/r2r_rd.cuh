@@ -81,13 +81,7 @@ __device__ __forceinline__ void rd_fft(cpx<T> (&v)[RdInfo<N>::R0],
         // X_N = 0; DST-III reads the line reversed.  X_{N-p} comes from the partner lane (or
         // the thread itself in warp 0); each pair of points is rewritten in place together so
         // only one array stays live.
-        auto ztw = [&](int q, cpx<T> xa, cpx<T> xb) -> cpx<T> {
-            const cpx<T> hh = ht[j + q * R1];
-            const T cc = hh.x, ss = hh.y;
-            const T var = cc * xa.x + ss * xb.x, vai = ss * xa.x - cc * xb.x;
-            const T vbr = cc * xa.y + ss * xb.y, vbi = ss * xa.y - cc * xb.y;
-            return {var - vbi, vai + vbr};
-        };
+        auto ztw = [&](int q, cpx<T> xa, cpx<T> xb) -> cpx<T> { return dct3_pre(xa, xb, ht[j + q * R1]); };
         if constexpr (ZMAP) {
             // butterfly j >= 1: partner point of q is R0 - 1 - q in butterfly R1 - j (lane pl;
             // j = R1/2 reads itself); butterfly 0 keeps its values for the path below
@@ -194,11 +188,7 @@ __device__ __forceinline__ void rd_fft(cpx<T> (&v)[RdInfo<N>::R0],
             // X[N - k] is block R1 - j at q' = R1 - 1 - q (lane ^ 16, or this thread for
             // j = R1/2), or block 0 at q' = (R1 - q) mod R1 for j = 0; each pair (q, q') is
             // rewritten in place together
-            auto post = [&](int q, cpx<T> zm) -> cpx<T> {
-                const int kk = j + R0 * q;
-                const cpx<T> hh = ht[kk];
-                return {dct2_out(x1[0][q], zm, hh, 0), dct2_out(x1[0][q], zm, hh, 1)};
-            };
+            auto post = [&](int q, cpx<T> zm) -> cpx<T> { return dct2_post(x1[0][q], zm, ht[j + R0 * q]); };
             if constexpr (ZMAP) {
                 const int lane = threadIdx.x & 31;
                 const int pl = j == 0 ? lane : lane + R1 - 2 * j;
@@ -276,9 +266,7 @@ __device__ __forceinline__ void rd_fft(cpx<T> (&v)[RdInfo<N>::R0],
                     const int kk = j + r * R1 + R0 * q;
                     const int km = kk == 0 ? 0 : N - kk;
                     const cpx<T> zm = line[RI::phys((km % R0) * R1 + km / R0)];
-                    const cpx<T> hh = ht[kk];
-                    const cpx<T> zk = x1[r][q];
-                    x1[r][q] = {dct2_out(zk, zm, hh, 0), dct2_out(zk, zm, hh, 1)};
+                    x1[r][q] = dct2_post(x1[r][q], zm, ht[kk]);
                 }
         }
     }
