@@ -44,9 +44,9 @@ CFG = dict(nw=8.0, dt=0.01, eps=-0.75, nu=1.0, alpha=1.0, beta=2.0, gamma=1.0)
 ERR_STEPS = 10000   # steps after which the FP32 psi is compared with the FP64 psi
 F_ADV = 32          # compulsory full-field transfers per adv step (single-sweep stages)
 # the kernel the roofline object describes, its key in pass_kernels and its ncu summary
-DOMINANT_PASS = "z_dct3"
-DOMINANT_PROFILE = "r2r_rdz_z_pass_dct3_256cube_fp32.md"
-DOMINANT_KERNEL = ("r2r_rdz_kernel<float,256,DCT-III> plain inverse pass along z (the largest share of the adv "
+DOMINANT_PASS = "x_dct3"
+DOMINANT_PROFILE = "r2r_rd_x_pass_dct3_256cube_fp32.md"
+DOMINANT_KERNEL = ("r2r_rd_kernel<float,256,x,DCT-III> plain inverse pass along x (the largest share of the adv "
                    "step's device time); algorithmic bytes per launch = 2 x 4 B x 256^3, 6-field ring")
 
 
