@@ -119,6 +119,7 @@ struct Ctx {
     int num_sms = 148;             // persistent grids (GEMM-form passes): one CTA per SM
     int *gz_err = nullptr;         // device word: nonzero when a GEMM-form pass gave up a bounded wait
     bool use_tma = false;          // FP32 plain strided passes fed by TMA, persistent (SMADFT_TMA_PASS=1)
+    bool stokes_true_k = true;     // adv: force spectra stored by true wavenumber, aligned Stokes reads (SMADFT_STOKES_K=0: not)
     bool share_grad = true;        // adv: gradients reuse psi's y and z passes (SMADFT_SHARE_GRAD=0: not)
     int grid_y = 1;                // strided and generic passes: CTA rows (fields of a batch group, LoadArrM)
     bool pooled = false;           // field slots live in a batch group's pools (the batch frees them)
@@ -315,7 +316,7 @@ int launch_fast(Ctx &c, int kind, LD ld, ST st)
 
 // plain z pass of length N through the register-direct z kernel (in == out allowed); with
 // zs, the pass of the shifted gradient spectrum along z (in != out)
-template <typename T, int N, int KIND, bool STAGE = false, bool GRADZ = false>
+template <typename T, int N, int KIND, bool STAGE = false, int ZM = kZPlain>
 int launch_rdz_k(Ctx &c, int kind, const T *in, T *out, const T *zs = nullptr)
 {
     const PlanDev &pd = c.plans.at(N);
@@ -326,12 +327,12 @@ int launch_rdz_k(Ctx &c, int kind, const T *in, T *out, const T *zs = nullptr)
     {
         std::lock_guard<std::mutex> lock(attr_mutex());
         if (!(attr_set >> (c.dev % kMaxDevices) & 1ull)) {
-            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N, KIND, STAGE, GRADZ>,
+            SMADFT_CUDA(cudaFuncSetAttribute(r2r_rdz_kernel<T, N, KIND, STAGE, ZM>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr_set |= 1ull << (c.dev % kMaxDevices);
         }
     }
-    r2r_rdz_kernel<T, N, KIND, STAGE, GRADZ><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
+    r2r_rdz_kernel<T, N, KIND, STAGE, ZM><<<(unsigned)tiles, RdInfo<N>::THREADS, smem, c.stream>>>(
         rows, kind, in, out, reinterpret_cast<const cpx<T> *>(pd.w), reinterpret_cast<const cpx<T> *>(pd.h),
         c.rdz_rev ? 1 : 0, zs);
     SMADFT_CUDA(cudaGetLastError());
@@ -363,8 +364,23 @@ int launch_rdz(Ctx &c, int kind, const T *in, T *out)
 template <typename T, int N>
 int launch_rdz_gradz(Ctx &c, const T *in, T *out, const T *zs)
 {
-    if (((uintptr_t)out & 15) == 0 && c.rdz_stage) return launch_rdz_k<T, N, K_DST3, true, true>(c, K_DST3, in, out, zs);
-    return launch_rdz_k<T, N, K_DST3, false, true>(c, K_DST3, in, out, zs);
+    if (((uintptr_t)out & 15) == 0 && c.rdz_stage) return launch_rdz_k<T, N, K_DST3, true, kZGrad>(c, K_DST3, in, out, zs);
+    return launch_rdz_k<T, N, K_DST3, false, kZGrad>(c, K_DST3, in, out, zs);
+}
+
+// inverse sine z pass of a spectrum stored by true wavenumber along z (read one index up)
+template <typename T, int N>
+int launch_rdz_upread(Ctx &c, const T *in, T *out)
+{
+    if (((uintptr_t)out & 15) == 0 && c.rdz_stage) return launch_rdz_k<T, N, K_DST3, true, kZUpRead>(c, K_DST3, in, out);
+    return launch_rdz_k<T, N, K_DST3, false, kZUpRead>(c, K_DST3, in, out);
+}
+
+// forward sine z pass whose output is stored by true wavenumber along z (one index up)
+template <typename T, int N>
+int launch_rdz_upstore(Ctx &c, const T *in, T *out)
+{
+    return launch_rdz_k<T, N, K_DST2, false, kZUpStore>(c, K_DST2, in, out);
 }
 
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link

@@ -95,6 +95,29 @@ int z_pass_grad(Ctx &c, const Spec<T> &s, const T *f, T *out)
     return launch_axis<T, 2>(c, K_DST3, LdGrad<T, 2, T>{s, f}, StoreArr<T>{out});
 }
 
+// sine z passes of spectra stored by true wavenumber along z (lengths with the register-direct
+// z kernel): the inverse one reads one index up, the forward one stores one index up
+template <typename T>
+int z_pass_upread(Ctx &c, const T *in, T *out)
+{
+    switch (c.g.nz) {
+    case 64: return launch_rdz_upread<T, 64>(c, in, out);
+    case 128: return launch_rdz_upread<T, 128>(c, in, out);
+    case 256: return launch_rdz_upread<T, 256>(c, in, out);
+    default: c.err = "z_pass_upread: length without the register-direct z kernel"; return SMADFT_ERR_INVALID;
+    }
+}
+template <typename T>
+int z_pass_upstore(Ctx &c, const T *in, T *out)
+{
+    switch (c.g.nz) {
+    case 64: return launch_rdz_upstore<T, 64>(c, in, out);
+    case 128: return launch_rdz_upstore<T, 128>(c, in, out);
+    case 256: return launch_rdz_upstore<T, 256>(c, in, out);
+    default: c.err = "z_pass_upstore: length without the register-direct z kernel"; return SMADFT_ERR_INVALID;
+    }
+}
+
 // -L(q) psihat (adv/cosAdvTrackMult.cpp:980-986)
 template <typename T>
 struct LdNegLin {
@@ -211,6 +234,78 @@ struct LdStokes {
                 const T dot = qi * sx + qj * sy + sk * szv[u];
                 T v = snu * inv * (szv[u] - sk * inv * dot);
                 if (DIVV) v = v + snu * inv * (s.nu * sk * dv[qk1]);
+                out[u] = (live && kl) ? v : T(0);
+            }
+        }
+    }
+};
+
+// The same projection from force spectra stored by true wavenumber: S~_c(I, J, K) is S_c with
+// the sine index of axis c moved up by one (S~_c = 0 at wavenumber 0 of axis c), so the three
+// values of one wavenumber sit at one index and every read is an aligned vector.  The
+// neighbours of LdStokes become S~x[i+1,j,k], S~y[i+1,j,k], S~z[i+1,j,k] (= Sx, Sy[i+1,j-1,k],
+// Sz[i+1,j,k-1]) for v_x and S~[i,j+1,k] for v_y; v_z is produced at its true wavenumber
+// (index k = wavenumber K) and its sine z pass reads it one index up.  Same operands, same
+// operations and truncations as LdStokes.
+template <typename T, int AX>
+struct LdStokesK {
+    Spec<T> s;
+    const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz;
+    template <int V>
+    __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
+    {
+        const T snu = s.scale / s.nu;
+        if (AX == 0) {
+            const bool live = i < s.nx - 1;
+            const idx_t qn = live ? q + s.nyz : q;         // wavenumber (i+1, j, k)
+            T sx[V], sy[V], sz[V];
+            vld<T, V>(Sx, qn, sx);
+            vld<T, V>(Sy, qn, sy);
+            vld<T, V>(Sz, qn, sz);
+            const T si = s.sx[i], qj = s.qy[j];
+            const T a2 = si * si + qj * qj;
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const T qk = s.qz[k + u];
+                const T inv = recip<T>(a2 + qk * qk);
+                const T dot = si * sx[u] + qj * sy[u] + qk * sz[u];
+                const T v = snu * inv * (sx[u] - si * inv * dot);
+                out[u] = live ? v : T(0);
+            }
+        } else if (AX == 1) {
+            const bool live = j < s.ny - 1;
+            const idx_t qj1 = live ? q + s.nz : q;          // wavenumber (i, j+1, k)
+            T sx[V], sy[V], sz[V];
+            vld<T, V>(Sx, qj1, sx);
+            vld<T, V>(Sy, qj1, sy);
+            vld<T, V>(Sz, qj1, sz);
+            const T qi = s.qx[i], sj = s.sy[j];
+            const T a2 = qi * qi + sj * sj;
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const int kk = k + u;
+                const T qk = s.qz[kk];
+                const T inv = recip<T>(a2 + qk * qk);
+                const T dot = qi * sx[u] + sj * sy[u] + qk * sz[u];
+                const T v = snu * inv * (sy[u] - sj * inv * dot);
+                out[u] = (live && kk < s.nz - 1) ? v : T(0);
+            }
+        } else {
+            const bool live = j < s.ny - 1;
+            T sx[V], sy[V], sz[V];
+            vld<T, V>(Sx, q, sx);
+            vld<T, V>(Sy, q, sy);
+            vld<T, V>(Sz, q, sz);
+            const T qi = s.qx[i], qj = s.qy[j];
+            const T a2 = qi * qi + qj * qj;
+#pragma unroll
+            for (int u = 0; u < V; u++) {
+                const int kk = k + u;                        // wavenumber K; sine index K - 1
+                const bool kl = kk >= 1;
+                const T sk = s.sz[kl ? kk - 1 : 0];
+                const T inv = recip<T>(a2 + sk * sk);
+                const T dot = qi * sx[u] + qj * sy[u] + sk * sz[u];
+                const T v = snu * inv * (sz[u] - sk * inv * dot);
                 out[u] = (live && kl) ? v : T(0);
             }
         }

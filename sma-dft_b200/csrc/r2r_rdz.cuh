@@ -31,9 +31,15 @@ constexpr size_t rdz_smem_bytes() { return rd_smem_bytes<T, N>() + (size_t)N * s
 // STAGE: the outputs go through shared memory and leave as whole rows in 16-byte stores (the
 // inverse kinds' Makhoul order would otherwise scatter every warp store over every second
 // element); `out` must then be 16-byte aligned.
-// GRADZ: the line read is the index-shifted gradient spectrum of `in` along z (LdGrad along
-// z): point n takes -zs[n] in[n + 1], and the last point 0; `out` must then differ from `in`.
-template <typename T, int N, int KIND = -1, bool STAGE = false, bool GRADZ = false>
+// ZM: how the line is read or written.  kZPlain; kZGrad: the index-shifted gradient spectrum
+// of `in` along z (LdGrad along z): point n takes -zs[n] in[n + 1], the last point 0;
+// kZUpRead: point n takes in[n + 1], the last point 0 (a spectrum stored by true wavenumber,
+// read as a sine series); kZUpStore (direct stores only): output position n goes to n + 1,
+// the last one is dropped and position 0 is zero-filled (a sine-axis spectrum stored by true
+// wavenumber).  Loads finish before the first barrier and a row belongs to one CTA, so every
+// mode may run in place.
+enum : int { kZPlain = 0, kZGrad = 1, kZUpRead = 2, kZUpStore = 3 };
+template <typename T, int N, int KIND = -1, bool STAGE = false, int ZM = kZPlain>
 __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2r_rdz_kernel(int rows, int kind_rt, const T *in, T *out,
                                                                         const cpx<T> *__restrict__ wt_g,
                                                                         const cpx<T> *__restrict__ ht_g, int rev,
@@ -70,12 +76,18 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     for (int q = 0; q < R0; q++) {
         const int n = pos.src(q);
         T a, b;
-        if constexpr (GRADZ) {
+        if constexpr (ZM == kZGrad) {
             const bool inr = n < N - 1;
             const int m = inr ? n + 1 : n;
             const T sc = inr ? -zs[n] : T(0);
             a = sc * pa[m];
             b = sc * pb[m];
+        } else if constexpr (ZM == kZUpRead) {
+            const bool inr = n < N - 1;
+            const int m = inr ? n + 1 : n;
+            const T ra = pa[m], rb = pb[m];
+            a = inr ? ra : T(0);
+            b = inr ? rb : T(0);
         } else {
             a = pa[n];
             b = pb[n];
@@ -91,6 +103,7 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
     __syncthreads();                                 // twiddle tables
     cpx<T> x1[BPT][R1];
     rd_fft<T, N, true>(v, x1, buf + c * RI::LD, wt, ht, j, threadIdx.x >> 5, fwd, sine, wz);
+    static_assert(!(STAGE && ZM == kZUpStore), "shifted stores go direct");
     if constexpr (STAGE) {
         // the CTA's 2 kRdLines rows in shared memory (inside the exchange buffer), then rows
         // of N elements out with 16-byte stores; rows past `rows` are not written
@@ -136,8 +149,15 @@ __global__ void __launch_bounds__(RdInfo<N>::THREADS, sizeof(T) == 4 ? 3 : 2) r2
         for (int pnt = 0; pnt < NP; pnt++) {
             const cpx<T> z = x1[pnt / R1][pnt % R1];
             const int o = pos.out(pnt);
-            if (oka) qa[o] = z.x;
-            if (okb) qb[o] = z.y;
+            if constexpr (ZM == kZUpStore) {
+                if (oka && o + 1 < N) qa[o + 1] = z.x;
+                if (okb && o + 1 < N) qb[o + 1] = z.y;
+                if (oka && o == 0) qa[0] = T(0);
+                if (okb && o == 0) qb[0] = T(0);
+            } else {
+                if (oka) qa[o] = z.x;
+                if (okb) qb[o] = z.y;
+            }
         }
     }
 }

@@ -509,6 +509,7 @@ int smadft_create(const smadft_params *p, smadft_ctx **out)
     // SMADFT_TMA_PASS=1: FP32 plain strided passes fed by TMA (r2r_rdt.cuh)
     if (const char *e = std::getenv("SMADFT_TMA_PASS")) c.use_tma = e[0] != '0';
     if (const char *e = std::getenv("SMADFT_SHARE_GRAD")) c.share_grad = e[0] != '0';
+    if (const char *e = std::getenv("SMADFT_STOKES_K")) c.stokes_true_k = e[0] != '0';
     auto bail = [&](int code) { smadft_destroy(h); return code; };
     if (cudaSetDevice(c.dev) != cudaSuccess) { cudaGetLastError(); delete h; return SMADFT_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SMADFT_ERR_CUDA);

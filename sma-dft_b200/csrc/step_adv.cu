@@ -37,6 +37,69 @@ int adv_psi_fields_shared(Ctx &c, const Spec<T> &s, const double *ph, T *psi, T 
     });
 }
 
+// The force spectra stored by true wavenumber, then the Stokes velocity from them (LdStokesK):
+// the sine-axis pass of each force component stores one index up along its axis (Sy in the
+// grouped y pass, Sz in its z pass, Sx in its x pass); the projection then reads the three
+// spectra of one wavenumber at one index, and v_z's sine z pass reads it one index up.  The
+// values and operations are those of the reference's indexing; only where they are stored
+// differs.  Needs the register-direct kernels on all three lengths.
+template <typename T>
+int adv_force_stokes_true_k(Ctx &c, const Spec<T> &s, T *psi, T *sp2, T *gx, T *gy, T *gz, T *Sx, T *Sy, T *Sz,
+                            T *vx, T *vy, T *vz)
+{
+    int rc;
+    {
+        const KindSet<3> ks{{K_DCT2, K_DST2, K_DCT2}};
+        const auto lm = make_multi(LdForce<T>{psi, sp2, gx, s.beta, s.gamma}, LdForce<T>{psi, sp2, gy, s.beta, s.gamma},
+                                   LdForce<T>{psi, sp2, gz, s.beta, s.gamma});
+        const StoreMultiUp<T, 3, 1> sm{{Sx, Sy, Sz}, 2u, (idx_t)c.g.nz, c.g.ny};
+        using LM = std::remove_const_t<decltype(lm)>;
+        using SM = StoreMultiUp<T, 3, 1>;
+        switch (c.g.ny) {
+        case 64: rc = launch_rd<T, 64, 1, LM, SM, 3, 1>(c, ks, lm, sm); break;
+        case 128: rc = launch_rd<T, 128, 1, LM, SM, 3, 1>(c, ks, lm, sm); break;
+        default: rc = launch_rd<T, 256, 1, LM, SM, 3, 1>(c, ks, lm, sm); break;
+        }
+        if (rc) return rc;
+        rc = forked(c, 3, [&](int m) {
+            int r;
+            switch (m) {
+            case 0:
+                if ((r = launch_axis<T, 2>(c, K_DCT2, LoadArr<T>{Sx}, StoreArr<T>{Sx}))) return r;
+                return launch_axis<T, 0>(c, K_DST2, LoadArr<T>{Sx}, StoreUp<T, 0>{Sx, (idx_t)c.g.nyz, c.g.nx});
+            case 1:
+                if ((r = launch_axis<T, 2>(c, K_DCT2, LoadArr<T>{Sy}, StoreArr<T>{Sy}))) return r;
+                return launch_axis<T, 0>(c, K_DCT2, LoadArr<T>{Sy}, StoreArr<T>{Sy});
+            default:
+                if ((r = z_pass_upstore<T>(c, Sz, Sz))) return r;
+                return launch_axis<T, 0>(c, K_DCT2, LoadArr<T>{Sz}, StoreArr<T>{Sz});
+            }
+        });
+        if (rc) return rc;
+    }
+    const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
+    T *const out[3] = {vx, vy, vz};
+    if ((rc = y_pass_multi<T, 3, 0>(c, ky, out, LdStokesK<T, 0>{s, Sx, Sy, Sz}, LdStokesK<T, 1>{s, Sx, Sy, Sz},
+                                    LdStokesK<T, 2>{s, Sx, Sy, Sz})))
+        return rc;
+    return forked(c, 3, [&](int m) {
+        int r;
+        switch (m) {
+        case 0:
+            if ((r = launch_axis<T, 2>(c, K_DCT3, LoadArr<T>{vx}, StoreArr<T>{vx}))) return r;
+            return launch_axis<T, 0>(c, K_DST3, LoadArr<T>{vx}, StoreArr<T>{vx});
+        case 1:
+            if ((r = launch_axis<T, 2>(c, K_DCT3, LoadArr<T>{vy}, StoreArr<T>{vy}))) return r;
+            return launch_axis<T, 0>(c, K_DCT3, LoadArr<T>{vy}, StoreArr<T>{vy});
+        default:
+            if ((r = z_pass_upread<T>(c, vz, vz))) return r;
+            return launch_axis<T, 0>(c, K_DCT3, LoadArr<T>{vz}, StoreArr<T>{vz});
+        }
+    });
+}
+
+inline bool rd_len(int n) { return n == 64 || n == 128 || n == 256; }
+
 // psi, grad psi, Sp2, the force spectra S-hat and the velocity v of the current psihat: the
 // loop body up to N (adv/cosAdvTrackMult.cpp:847-1286)
 template <typename T>
@@ -61,7 +124,10 @@ int adv_fields(Ctx &c)
                                     LdGrad<T, 1, double>{s, ph}, LdGrad<T, 2, double>{s, ph}, LdNegLin<T>{s, ph})))
             return rc;
     }
-    // force spectra S_c = ST_c(mu d_c psi) (:996-1027)
+    // force spectra S_c = ST_c(mu d_c psi) (:996-1027) and the Stokes velocity (:1030-1286)
+    if (c.stokes_true_k && c.use_rd && c.use_rdz && c.use_multi && !plane_ok(c) && rd_len(c.g.nx) &&
+        rd_len(c.g.ny) && rd_len(c.g.nz))
+        return adv_force_stokes_true_k<T>(c, s, psi, sp2, gx, gy, gz, Sx, Sy, Sz, vx, vy, vz);
     {
         const int kx[3] = {K_DST2, K_DCT2, K_DCT2};
         const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
