@@ -235,45 +235,104 @@ int adv_group_step(Ctx *const *mm, int M)
         for (int m = 0; m < 5; m++)
             if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
     }
-    // force spectra S_c = ST_c(mu d_c psi) (:996-1027)
-    {
-        const int kx[3] = {K_DST2, K_DCT2, K_DCT2};
-        const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
-        const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
-        const int slots[3] = {S_SX, S_SY, S_SZ};
+    // force spectra S_c = ST_c(mu d_c psi) (:996-1027) and the Stokes velocity (:1030-1286)
+    if (L.stokes_true_k && L.use_rd && L.use_rdz && L.use_multi && rd_len(L.g.nx) && rd_len(L.g.ny) &&
+        rd_len(L.g.nz)) {
+        // the order of adv_force_stokes_true_k: force spectra by true wavenumber, aligned
+        // projection; the z passes that store or read one index up run over the pool, Sx's
+        // x pass (one index up) per member
+        auto pz_up = [&](int slot, bool store) {
+            return on_pool_copy(L, [&](Ctx &pc) {
+                pc.g.nx = L.g.nx * M;
+#ifdef SMADFT_CHECK_BOUNDS
+                pc.g.nelem = L.g.nelem * M;
+#endif
+                T *f = L.f<T>(slot);
+                return store ? z_pass_upstore<T>(pc, f, f) : z_pass_upread<T>(pc, f, f);
+            });
+        };
         for (int i = 0; i < M; i++) {
             rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
                 Spec<T> s = make_spec<T>(c);
                 T *psi = c.f<T>(S_PSI), *sp2 = c.f<T>(S_SP2);
-                T *const out[3] = {c.f<T>(S_SX), c.f<T>(S_SY), c.f<T>(S_SZ)};
-                return y_pass_multi<T, 3, 1>(c, ky, out, LdForce<T>{psi, sp2, c.f<T>(S_GX), s.beta, s.gamma},
-                                             LdForce<T>{psi, sp2, c.f<T>(S_GY), s.beta, s.gamma},
-                                             LdForce<T>{psi, sp2, c.f<T>(S_GZ), s.beta, s.gamma});
+                const KindSet<3> ks{{K_DCT2, K_DST2, K_DCT2}};
+                const auto lm = make_multi(LdForce<T>{psi, sp2, c.f<T>(S_GX), s.beta, s.gamma},
+                                           LdForce<T>{psi, sp2, c.f<T>(S_GY), s.beta, s.gamma},
+                                           LdForce<T>{psi, sp2, c.f<T>(S_GZ), s.beta, s.gamma});
+                const StoreMultiUp<T, 3, 1> sm{{c.f<T>(S_SX), c.f<T>(S_SY), c.f<T>(S_SZ)}, 2u, (idx_t)c.g.nz, c.g.ny};
+                using LM = std::remove_const_t<decltype(lm)>;
+                using SM = StoreMultiUp<T, 3, 1>;
+                switch (c.g.ny) {
+                case 64: return launch_rd<T, 64, 1, LM, SM, 3, 1>(c, ks, lm, sm);
+                case 128: return launch_rd<T, 128, 1, LM, SM, 3, 1>(c, ks, lm, sm);
+                default: return launch_rd<T, 256, 1, LM, SM, 3, 1>(c, ks, lm, sm);
+                }
             });
             if (rc) return rc;
         }
-        for (int m = 0; m < 3; m++)
-            if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
-    }
-    // Stokes velocity (:1030-1286)
-    {
-        const int kx[3] = {K_DST3, K_DCT3, K_DCT3};
+        if ((rc = pz(S_SX, K_DCT2)) || (rc = pz(S_SY, K_DCT2)) || (rc = pz_up(S_SZ, true))) return rc;
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                T *Sx = c.f<T>(S_SX);
+                return launch_axis<T, 0>(c, K_DST2, LoadArr<T>{Sx}, StoreUp<T, 0>{Sx, (idx_t)c.g.nyz, c.g.nx});
+            });
+            if (rc) return rc;
+        }
+        if ((rc = px(S_SY, K_DCT2)) || (rc = px(S_SZ, K_DCT2))) return rc;
         const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
-        const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
-        const int slots[3] = {S_VX, S_VY, S_VZ};
         for (int i = 0; i < M; i++) {
             rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
                 Spec<T> s = make_spec<T>(c);
                 T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
                 T *const out[3] = {c.f<T>(S_VX), c.f<T>(S_VY), c.f<T>(S_VZ)};
-                return y_pass_multi<T, 3, 0>(c, ky, out, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr},
-                                             LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr},
-                                             LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr});
+                return y_pass_multi<T, 3, 0>(c, ky, out, LdStokesK<T, 0>{s, Sx, Sy, Sz}, LdStokesK<T, 1>{s, Sx, Sy, Sz},
+                                             LdStokesK<T, 2>{s, Sx, Sy, Sz});
             });
             if (rc) return rc;
         }
-        for (int m = 0; m < 3; m++)
-            if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
+        if ((rc = pz(S_VX, K_DCT3)) || (rc = px(S_VX, K_DST3)) || (rc = pz(S_VY, K_DCT3)) ||
+            (rc = px(S_VY, K_DCT3)) || (rc = pz_up(S_VZ, false)) || (rc = px(S_VZ, K_DCT3)))
+            return rc;
+    } else {
+        {
+            const int kx[3] = {K_DST2, K_DCT2, K_DCT2};
+            const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
+            const int kz[3] = {K_DCT2, K_DCT2, K_DST2};
+            const int slots[3] = {S_SX, S_SY, S_SZ};
+            for (int i = 0; i < M; i++) {
+                rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                    Spec<T> s = make_spec<T>(c);
+                    T *psi = c.f<T>(S_PSI), *sp2 = c.f<T>(S_SP2);
+                    T *const out[3] = {c.f<T>(S_SX), c.f<T>(S_SY), c.f<T>(S_SZ)};
+                    return y_pass_multi<T, 3, 1>(c, ky, out, LdForce<T>{psi, sp2, c.f<T>(S_GX), s.beta, s.gamma},
+                                                 LdForce<T>{psi, sp2, c.f<T>(S_GY), s.beta, s.gamma},
+                                                 LdForce<T>{psi, sp2, c.f<T>(S_GZ), s.beta, s.gamma});
+                });
+                if (rc) return rc;
+            }
+            for (int m = 0; m < 3; m++)
+                if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
+        }
+        // Stokes velocity (:1030-1286)
+        {
+            const int kx[3] = {K_DST3, K_DCT3, K_DCT3};
+            const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
+            const int kz[3] = {K_DCT3, K_DCT3, K_DST3};
+            const int slots[3] = {S_VX, S_VY, S_VZ};
+            for (int i = 0; i < M; i++) {
+                rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                    Spec<T> s = make_spec<T>(c);
+                    T *Sx = c.f<T>(S_SX), *Sy = c.f<T>(S_SY), *Sz = c.f<T>(S_SZ);
+                    T *const out[3] = {c.f<T>(S_VX), c.f<T>(S_VY), c.f<T>(S_VZ)};
+                    return y_pass_multi<T, 3, 0>(c, ky, out, LdStokes<T, 0, false>{s, Sx, Sy, Sz, nullptr},
+                                                 LdStokes<T, 1, false>{s, Sx, Sy, Sz, nullptr},
+                                                 LdStokes<T, 2, false>{s, Sx, Sy, Sz, nullptr});
+                });
+                if (rc) return rc;
+            }
+            for (int m = 0; m < 3; m++)
+                if ((rc = pz(slots[m], kz[m])) || (rc = px(slots[m], kx[m]))) return rc;
+        }
     }
     // N = beta psi^3 - gamma psi^5 - v.grad psi into the scratch field, CN/AB2 update (:1290-1365)
     for (int i = 0; i < M; i++) {

@@ -69,3 +69,29 @@ def test_true_k_stokes_matches_oracle(prec, monkeypatch):
         err = np.linalg.norm(got[f] - want) / np.linalg.norm(want)
         print(f"{f}: rel L2 vs oracle {err:.2e}")
         assert err <= tol, f
+
+
+@pytest.mark.parametrize("prec", [smadft.FP64, smadft.FP32], ids=["fp64", "fp32"])
+def test_true_k_stokes_in_batch_groups_matches_solo_runs(prec):
+    """A batch group of adv members runs the same order with its z passes over the pool."""
+    cases = [smadft.params(smadft.ADV, (64, 64, 64), precision=prec, dt=0.01, eps=-0.7 - 0.05 * i) for i in range(2)]
+    ics = [smadft.ic_conics(p, A=1.3, count=2, rmin=1.0, rmax=2.0, noise=1e-3, seed=40 + i)
+           for i, p in enumerate(cases)]
+    solo = []
+    for p, ic in zip(cases, ics):
+        with smadft.Solver(p) as s:
+            s.set_psi(ic)
+            s.step(5)
+            solo.append({f: s.get(f) for f in ("psi", "vx", "vy", "vz")})
+    with smadft.Batch(cases) as b:
+        assert b.groups == 1
+        for i, ic in enumerate(ics):
+            b.members[i].set_psi(ic)
+        b.step(5)
+        b.sync()
+        for i in range(len(cases)):
+            for f in ("psi", "vx", "vy", "vz"):
+                got, want = b.members[i].get(f), solo[i][f]
+                d = np.linalg.norm(got - want) / np.linalg.norm(want)
+                print(f"member {i} {f}: group vs solo {d:.2e}")
+                assert d <= (1e-12 if prec == smadft.FP64 else 1e-5), (i, f)
