@@ -240,66 +240,62 @@ struct LdStokes {
     }
 };
 
-// The same projection with Sz stored by true wavenumber: S~z(i, j, K) is Sz with its sine
-// index along z moved up by one (S~z = 0 at K = 0), so its neighbour Sz[.., k-1] sits at k and
-// every read is an aligned vector; the x and y neighbours are whole planes or rows away
-// (aligned already).  v_x and v_y come out at their sine indices; v_z is produced at its
-// true wavenumber (index k = wavenumber K) and its sine z pass reads it one index up.  Same
-// operands, operations and truncations as LdStokes.
+// The same projection from force spectra stored by true wavenumber: S~_c(I, J, K) is S_c with
+// the sine index of axis c moved up by one (S~_c = 0 at wavenumber 0 of axis c), so the three
+// values of one wavenumber sit at one index and every read is an aligned vector.  The
+// neighbours of LdStokes become S~x[i+1,j,k], S~y[i+1,j,k], S~z[i+1,j,k] (= Sx, Sy[i+1,j-1,k],
+// Sz[i+1,j,k-1]) for v_x and S~[i,j+1,k] for v_y; v_z is produced at its true wavenumber
+// (index k = wavenumber K) and its sine z pass reads it one index up.  Same operands, same
+// operations and truncations as LdStokes.
 template <typename T, int AX>
 struct LdStokesK {
     Spec<T> s;
-    const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz;   // Sz by true wavenumber along z
+    const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz;
     template <int V>
     __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         const T snu = s.scale / s.nu;
         if (AX == 0) {
             const bool live = i < s.nx - 1;
-            const idx_t qn = live ? q + s.nyz : q;         // (i+1, j, k)
-            const bool jy = j != 0;
+            const idx_t qn = live ? q + s.nyz : q;         // wavenumber (i+1, j, k)
             T sx[V], sy[V], sz[V];
-            vld<T, V>(Sx, q, sx);
-            vld<T, V>(Sy, jy ? qn - s.nz : qn, sy);         // Sy[i+1, j-1, k]
-            vld<T, V>(Sz, qn, sz);                          // Sz[i+1, j, k-1]
+            vld<T, V>(Sx, qn, sx);
+            vld<T, V>(Sy, qn, sy);
+            vld<T, V>(Sz, qn, sz);
             const T si = s.sx[i], qj = s.qy[j];
             const T a2 = si * si + qj * qj;
 #pragma unroll
             for (int u = 0; u < V; u++) {
                 const T qk = s.qz[k + u];
-                const T syv = jy ? sy[u] : T(0);
                 const T inv = recip<T>(a2 + qk * qk);
-                const T dot = si * sx[u] + qj * syv + qk * sz[u];
+                const T dot = si * sx[u] + qj * sy[u] + qk * sz[u];
                 const T v = snu * inv * (sx[u] - si * inv * dot);
                 out[u] = live ? v : T(0);
             }
         } else if (AX == 1) {
             const bool live = j < s.ny - 1;
-            const idx_t qj1 = live ? q + s.nz : q;          // (i, j+1, k)
-            const bool ix = i != 0;
+            const idx_t qj1 = live ? q + s.nz : q;          // wavenumber (i, j+1, k)
             T sx[V], sy[V], sz[V];
-            vld<T, V>(Sy, q, sy);
-            vld<T, V>(Sx, ix ? qj1 - s.nyz : qj1, sx);      // Sx[i-1, j+1, k]
-            vld<T, V>(Sz, qj1, sz);                         // Sz[i, j+1, k-1]
+            vld<T, V>(Sx, qj1, sx);
+            vld<T, V>(Sy, qj1, sy);
+            vld<T, V>(Sz, qj1, sz);
             const T qi = s.qx[i], sj = s.sy[j];
             const T a2 = qi * qi + sj * sj;
 #pragma unroll
             for (int u = 0; u < V; u++) {
                 const int kk = k + u;
                 const T qk = s.qz[kk];
-                const T sxv = ix ? sx[u] : T(0);
                 const T inv = recip<T>(a2 + qk * qk);
-                const T dot = qi * sxv + sj * sy[u] + qk * sz[u];
+                const T dot = qi * sx[u] + sj * sy[u] + qk * sz[u];
                 const T v = snu * inv * (sy[u] - sj * inv * dot);
                 out[u] = (live && kk < s.nz - 1) ? v : T(0);
             }
         } else {
             const bool live = j < s.ny - 1;
-            const bool ix = i != 0, jy = j != 0;
             T sx[V], sy[V], sz[V];
-            vld<T, V>(Sx, ix ? q - s.nyz : q, sx);          // Sx[i-1, j, K]
-            vld<T, V>(Sy, jy ? q - s.nz : q, sy);           // Sy[i, j-1, K]
-            vld<T, V>(Sz, q, sz);                           // Sz[i, j, K-1]
+            vld<T, V>(Sx, q, sx);
+            vld<T, V>(Sy, q, sy);
+            vld<T, V>(Sz, q, sz);
             const T qi = s.qx[i], qj = s.qy[j];
             const T a2 = qi * qi + qj * qj;
 #pragma unroll
@@ -307,9 +303,8 @@ struct LdStokesK {
                 const int kk = k + u;                        // wavenumber K; sine index K - 1
                 const bool kl = kk >= 1;
                 const T sk = s.sz[kl ? kk - 1 : 0];
-                const T sxv = ix ? sx[u] : T(0), syv = jy ? sy[u] : T(0);
                 const T inv = recip<T>(a2 + sk * sk);
-                const T dot = qi * sxv + qj * syv + sk * sz[u];
+                const T dot = qi * sx[u] + qj * sy[u] + sk * sz[u];
                 const T v = snu * inv * (sz[u] - sk * inv * dot);
                 out[u] = (live && kl) ? v : T(0);
             }

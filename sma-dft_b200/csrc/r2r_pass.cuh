@@ -317,6 +317,69 @@ struct StoreMulti {
     }
 };
 
+// Position along the line of a pass along AXIS, and stores one index up along it: output
+// position t goes to t + 1 (`stride` elements further), the last position (t = n - 1) is
+// dropped and position 0 is zero-filled.  Spectra of a sine axis stored this way sit at
+// their true wavenumber (sine index t is wavenumber t + 1).
+template <int AXIS>
+__device__ __forceinline__ int line_pos(int i, int j, int k) { return AXIS == 0 ? i : AXIS == 1 ? j : k; }
+template <typename T, int V>
+__device__ __forceinline__ void vst_up(T *p, idx_t idx, idx_t stride, int t, int n, const T *v)
+{
+    if (t + 1 < n) vst<T, V>(p, idx + stride, v);
+    if (t == 0) {
+        T z[V];
+#pragma unroll
+        for (int u = 0; u < V; u++) z[u] = T(0);
+        vst<T, V>(p, idx, z);
+    }
+}
+
+// StoreMulti whose components in `up` (bit c) store one index up along the pass's line axis
+template <typename T, int NC, int AXIS>
+struct StoreMultiUp {
+    static constexpr bool MULTI = true;
+    T *p[NC];
+    unsigned up;
+    idx_t stride;
+    int n;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(int, idx_t, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void store(int comp, idx_t idx, int i, int j, int k, const T *v) const
+    {
+        if (up >> comp & 1u) vst_up<T, V>(p[comp], idx, stride, line_pos<AXIS>(i, j, k), n, v);
+        else vst<T, V>(p[comp], idx, v);
+    }
+    template <int V>
+    __device__ __forceinline__ void fin(int comp, idx_t idx, int i, int j, int k, const T *v, const T *) const
+    {
+        store<V>(comp, idx, i, j, k, v);
+    }
+};
+
+// one field stored one index up along the pass's line axis (see vst_up)
+template <typename T, int AXIS>
+struct StoreUp {
+    T *p;
+    idx_t stride;
+    int n;
+    static constexpr int PRE = 0;
+    template <int V>
+    __device__ __forceinline__ void pre(idx_t, int, int, int, T *) const {}
+    template <int V>
+    __device__ __forceinline__ void store(idx_t idx, int i, int j, int k, const T *v) const
+    {
+        vst_up<T, V>(p, idx, stride, line_pos<AXIS>(i, j, k), n, v);
+    }
+    template <int V>
+    __device__ __forceinline__ void fin(idx_t idx, int i, int j, int k, const T *v, const T *) const
+    {
+        store<V>(idx, i, j, k, v);
+    }
+};
+
 // per-component transform kind of a multi-component pass
 template <int NC>
 struct KindSet {

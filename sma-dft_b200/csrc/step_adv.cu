@@ -37,29 +37,36 @@ int adv_psi_fields_shared(Ctx &c, const Spec<T> &s, const double *ph, T *psi, T 
     });
 }
 
-// The force spectra with Sz stored by true wavenumber along z, then the Stokes velocity from
-// them (LdStokesK): Sz's sine z pass stores one index up, so the projection reads every
-// neighbour as an aligned vector, and v_z's sine z pass reads it one index up.  The values
-// and operations are those of the reference's indexing; only where Sz and v_z are stored in
-// between differs.  Needs the register-direct kernels on all three lengths.
+// The force spectra stored by true wavenumber, then the Stokes velocity from them (LdStokesK):
+// the sine-axis pass of each force component stores one index up along its axis (Sy in the
+// grouped y pass, Sz in its z pass, Sx in its x pass); the projection then reads the three
+// spectra of one wavenumber at one index, and v_z's sine z pass reads it one index up.  The
+// values and operations are those of the reference's indexing; only where they are stored
+// differs.  Needs the register-direct kernels on all three lengths.
 template <typename T>
 int adv_force_stokes_true_k(Ctx &c, const Spec<T> &s, T *psi, T *sp2, T *gx, T *gy, T *gz, T *Sx, T *Sy, T *Sz,
                             T *vx, T *vy, T *vz)
 {
     int rc;
     {
-        const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
-        T *const out[3] = {Sx, Sy, Sz};
-        if ((rc = y_pass_multi<T, 3, 1>(c, ky, out, LdForce<T>{psi, sp2, gx, s.beta, s.gamma},
-                                        LdForce<T>{psi, sp2, gy, s.beta, s.gamma},
-                                        LdForce<T>{psi, sp2, gz, s.beta, s.gamma})))
-            return rc;
+        const KindSet<3> ks{{K_DCT2, K_DST2, K_DCT2}};
+        const auto lm = make_multi(LdForce<T>{psi, sp2, gx, s.beta, s.gamma}, LdForce<T>{psi, sp2, gy, s.beta, s.gamma},
+                                   LdForce<T>{psi, sp2, gz, s.beta, s.gamma});
+        const StoreMultiUp<T, 3, 1> sm{{Sx, Sy, Sz}, 2u, (idx_t)c.g.nz, c.g.ny};
+        using LM = std::remove_const_t<decltype(lm)>;
+        using SM = StoreMultiUp<T, 3, 1>;
+        switch (c.g.ny) {
+        case 64: rc = launch_rd<T, 64, 1, LM, SM, 3, 1>(c, ks, lm, sm); break;
+        case 128: rc = launch_rd<T, 128, 1, LM, SM, 3, 1>(c, ks, lm, sm); break;
+        default: rc = launch_rd<T, 256, 1, LM, SM, 3, 1>(c, ks, lm, sm); break;
+        }
+        if (rc) return rc;
         rc = forked(c, 3, [&](int m) {
             int r;
             switch (m) {
             case 0:
                 if ((r = launch_axis<T, 2>(c, K_DCT2, LoadArr<T>{Sx}, StoreArr<T>{Sx}))) return r;
-                return launch_axis<T, 0>(c, K_DST2, LoadArr<T>{Sx}, StoreArr<T>{Sx});
+                return launch_axis<T, 0>(c, K_DST2, LoadArr<T>{Sx}, StoreUp<T, 0>{Sx, (idx_t)c.g.nyz, c.g.nx});
             case 1:
                 if ((r = launch_axis<T, 2>(c, K_DCT2, LoadArr<T>{Sy}, StoreArr<T>{Sy}))) return r;
                 return launch_axis<T, 0>(c, K_DCT2, LoadArr<T>{Sy}, StoreArr<T>{Sy});
@@ -231,8 +238,9 @@ int adv_group_step(Ctx *const *mm, int M)
     // force spectra S_c = ST_c(mu d_c psi) (:996-1027) and the Stokes velocity (:1030-1286)
     if (L.stokes_true_k && L.use_rd && L.use_rdz && L.use_multi && rd_len(L.g.nx) && rd_len(L.g.ny) &&
         rd_len(L.g.nz)) {
-        // the order of adv_force_stokes_true_k, with the z passes that store or read one
-        // index up run over the pool
+        // the order of adv_force_stokes_true_k: force spectra by true wavenumber, aligned
+        // projection; the z passes that store or read one index up run over the pool, Sx's
+        // x pass (one index up) per member
         auto pz_up = [&](int slot, bool store) {
             return on_pool_copy(L, [&](Ctx &pc) {
                 pc.g.nx = L.g.nx * M;
@@ -243,23 +251,34 @@ int adv_group_step(Ctx *const *mm, int M)
                 return store ? z_pass_upstore<T>(pc, f, f) : z_pass_upread<T>(pc, f, f);
             });
         };
-        {
-            const int ky[3] = {K_DCT2, K_DST2, K_DCT2};
-            for (int i = 0; i < M; i++) {
-                rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
-                    Spec<T> s = make_spec<T>(c);
-                    T *psi = c.f<T>(S_PSI), *sp2 = c.f<T>(S_SP2);
-                    T *const out[3] = {c.f<T>(S_SX), c.f<T>(S_SY), c.f<T>(S_SZ)};
-                    return y_pass_multi<T, 3, 1>(c, ky, out, LdForce<T>{psi, sp2, c.f<T>(S_GX), s.beta, s.gamma},
-                                                 LdForce<T>{psi, sp2, c.f<T>(S_GY), s.beta, s.gamma},
-                                                 LdForce<T>{psi, sp2, c.f<T>(S_GZ), s.beta, s.gamma});
-                });
-                if (rc) return rc;
-            }
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                Spec<T> s = make_spec<T>(c);
+                T *psi = c.f<T>(S_PSI), *sp2 = c.f<T>(S_SP2);
+                const KindSet<3> ks{{K_DCT2, K_DST2, K_DCT2}};
+                const auto lm = make_multi(LdForce<T>{psi, sp2, c.f<T>(S_GX), s.beta, s.gamma},
+                                           LdForce<T>{psi, sp2, c.f<T>(S_GY), s.beta, s.gamma},
+                                           LdForce<T>{psi, sp2, c.f<T>(S_GZ), s.beta, s.gamma});
+                const StoreMultiUp<T, 3, 1> sm{{c.f<T>(S_SX), c.f<T>(S_SY), c.f<T>(S_SZ)}, 2u, (idx_t)c.g.nz, c.g.ny};
+                using LM = std::remove_const_t<decltype(lm)>;
+                using SM = StoreMultiUp<T, 3, 1>;
+                switch (c.g.ny) {
+                case 64: return launch_rd<T, 64, 1, LM, SM, 3, 1>(c, ks, lm, sm);
+                case 128: return launch_rd<T, 128, 1, LM, SM, 3, 1>(c, ks, lm, sm);
+                default: return launch_rd<T, 256, 1, LM, SM, 3, 1>(c, ks, lm, sm);
+                }
+            });
+            if (rc) return rc;
         }
-        if ((rc = pz(S_SX, K_DCT2)) || (rc = px(S_SX, K_DST2)) || (rc = pz(S_SY, K_DCT2)) ||
-            (rc = px(S_SY, K_DCT2)) || (rc = pz_up(S_SZ, true)) || (rc = px(S_SZ, K_DCT2)))
-            return rc;
+        if ((rc = pz(S_SX, K_DCT2)) || (rc = pz(S_SY, K_DCT2)) || (rc = pz_up(S_SZ, true))) return rc;
+        for (int i = 0; i < M; i++) {
+            rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {
+                T *Sx = c.f<T>(S_SX);
+                return launch_axis<T, 0>(c, K_DST2, LoadArr<T>{Sx}, StoreUp<T, 0>{Sx, (idx_t)c.g.nyz, c.g.nx});
+            });
+            if (rc) return rc;
+        }
+        if ((rc = px(S_SY, K_DCT2)) || (rc = px(S_SZ, K_DCT2))) return rc;
         const int ky[3] = {K_DCT3, K_DST3, K_DCT3};
         for (int i = 0; i < M; i++) {
             rc = on_lead_stream(L, *mm[i], [&](Ctx &c) {

@@ -1,10 +1,12 @@
-"""Force spectrum Sz stored by true wavenumber and the aligned Stokes projection (LdStokesK).
+"""Force spectra stored by true wavenumber and the aligned Stokes projection (LdStokesK).
 
 With SMADFT_STOKES_K=1 (the default where all three lengths have the register-direct
-kernels) Sz's sine z pass stores its output one index up along z, the projection reads every
-operand as an aligned vector, and v_z's sine z pass reads its spectrum one index up.  The
-operands and operations are the reference-indexed ones (SMADFT_STOKES_K=0), so velocities and
-whole steps agree to rounding; both stay on the oracle's trajectory.
+kernels) the sine-axis pass of each force component stores its output one index up along
+its axis, the projection reads the three spectra of one wavenumber at one index, and v_z's
+sine z pass reads its spectrum one index up.  The operands and operations are the
+reference-indexed ones (SMADFT_STOKES_K=0), so velocities and whole steps agree to rounding
+(the passes that store or read one index up are separate instantiations of the same
+transforms); both stay on the oracle's trajectory.
 """
 import numpy as np
 import pytest
