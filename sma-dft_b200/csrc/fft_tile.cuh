@@ -79,6 +79,13 @@ __device__ __forceinline__ cpx<T> caxpy(cpx<T> a, T s, cpx<T> b) { return {fma(s
 template <typename T>
 __device__ __forceinline__ cpx<T> cscale(T s, cpx<T> b) { return {s * b.x, s * b.y}; }
 
+// lane-wise product and multiply-add of two pairs (a.x b.x, a.y b.y) and (a.x b.x + c.x, ...):
+// two independent real values carried as one pair (two points of a loader)
+template <typename T>
+__device__ __forceinline__ cpx<T> pmul(cpx<T> a, cpx<T> b) { return {a.x * b.x, a.y * b.y}; }
+template <typename T>
+__device__ __forceinline__ cpx<T> pfma(cpx<T> a, cpx<T> b, cpx<T> c) { return {fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)}; }
+
 __device__ __forceinline__ unsigned long long pk2(cpx<float> a)
 {
     unsigned long long r;
@@ -138,6 +145,21 @@ __device__ __forceinline__ cpx<T> dct2_post(cpx<T> zk, cpx<T> zm, cpx<T> h)
 {
     const cpx<T> p = cadd(zk, zm), d = csub(zk, zm);
     return {fma(h.y, d.y, h.x * p.x), fma(-h.y, d.x, h.x * p.y)};
+}
+
+template <>
+__device__ __forceinline__ cpx<float> pmul<float>(cpx<float> a, cpx<float> b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(r);
+}
+template <>
+__device__ __forceinline__ cpx<float> pfma<float>(cpx<float> a, cpx<float> b, cpx<float> c)
+{
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(c)));
+    return upk2(r);
 }
 
 // Size-R DFT in registers.  Forward uses exp(-2 pi i/R), inverse exp(+2 pi i/R).

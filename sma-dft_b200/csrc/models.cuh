@@ -251,10 +251,69 @@ template <typename T, int AX>
 struct LdStokesK {
     Spec<T> s;
     const T *__restrict__ Sx, *__restrict__ Sy, *__restrict__ Sz;
+    // v = snu inv (own - sc inv dot), inv = 1 / (a2 + qk^2), dot = c0 x + c1 y + qk z, for the
+    // two points of a pair at once (lane-wise packed arithmetic; the same operations in the
+    // same order as the scalar form)
+    __device__ __forceinline__ static cpx<T> proj2(T snu, T a2, T c0, T c1, T sc, cpx<T> qk, cpx<T> x, cpx<T> y,
+                                                   cpx<T> z, cpx<T> own)
+    {
+        const cpx<T> d = pfma(qk, qk, cpx<T>{a2, a2});
+        const cpx<T> inv{recip<T>(d.x), recip<T>(d.y)};
+        const cpx<T> dot = pfma(qk, z, pfma(cpx<T>{c1, c1}, y, pmul(cpx<T>{c0, c0}, x)));
+        const cpx<T> t = pfma(pmul(cpx<T>{-sc, -sc}, inv), dot, own);
+        return pmul(pmul(cpx<T>{snu, snu}, inv), t);
+    }
     template <int V>
     __device__ __forceinline__ void load(idx_t q, int i, int j, int k, T *out) const
     {
         const T snu = s.scale / s.nu;
+        if constexpr (V == 2) {
+            // k even: the pair (k, k+1) of every field and table is one aligned vector
+            T x[2], y[2], z[2];
+            if (AX == 0) {
+                const bool live = i < s.nx - 1;
+                const idx_t qn = live ? q + s.nyz : q;
+                vld<T, 2>(Sx, qn, x);
+                vld<T, 2>(Sy, qn, y);
+                vld<T, 2>(Sz, qn, z);
+                const T si = s.sx[i], qj = s.qy[j];
+                const cpx<T> X{x[0], x[1]};
+                const cpx<T> v = proj2(snu, si * si + qj * qj, si, qj, si, cpx<T>{s.qz[k], s.qz[k + 1]}, X,
+                                       cpx<T>{y[0], y[1]}, cpx<T>{z[0], z[1]}, X);
+                out[0] = live ? v.x : T(0);
+                out[1] = live ? v.y : T(0);
+            } else if (AX == 1) {
+                const bool live = j < s.ny - 1;
+                const idx_t qj1 = live ? q + s.nz : q;
+                vld<T, 2>(Sx, qj1, x);
+                vld<T, 2>(Sy, qj1, y);
+                vld<T, 2>(Sz, qj1, z);
+                const T qi = s.qx[i], sj = s.sy[j];
+                const cpx<T> Y{y[0], y[1]};
+                const cpx<T> v = proj2(snu, qi * qi + sj * sj, qi, sj, sj, cpx<T>{s.qz[k], s.qz[k + 1]},
+                                       cpx<T>{x[0], x[1]}, Y, cpx<T>{z[0], z[1]}, Y);
+                out[0] = (live && k < s.nz - 1) ? v.x : T(0);
+                out[1] = (live && k + 1 < s.nz - 1) ? v.y : T(0);
+            } else {
+                const bool live = j < s.ny - 1;
+                vld<T, 2>(Sx, q, x);
+                vld<T, 2>(Sy, q, y);
+                vld<T, 2>(Sz, q, z);
+                const T qi = s.qx[i], qj = s.qy[j];
+                const bool kl = k >= 1;
+                const cpx<T> sk{s.sz[kl ? k - 1 : 0], s.sz[k]};
+                const cpx<T> Z{z[0], z[1]};
+                // the sine wavenumber is the product's own coefficient here: dot = qi x + qj y + sk z
+                const cpx<T> d = pfma(sk, sk, cpx<T>{qi * qi + qj * qj, qi * qi + qj * qj});
+                const cpx<T> inv{recip<T>(d.x), recip<T>(d.y)};
+                const cpx<T> dot = pfma(sk, Z, pfma(cpx<T>{qj, qj}, cpx<T>{y[0], y[1]}, pmul(cpx<T>{qi, qi}, cpx<T>{x[0], x[1]})));
+                const cpx<T> t = pfma(pmul(cpx<T>{-sk.x, -sk.y}, inv), dot, Z);
+                const cpx<T> v = pmul(pmul(cpx<T>{snu, snu}, inv), t);
+                out[0] = (live && kl) ? v.x : T(0);
+                out[1] = live ? v.y : T(0);
+            }
+            return;
+        }
         if (AX == 0) {
             const bool live = i < s.nx - 1;
             const idx_t qn = live ? q + s.nyz : q;         // wavenumber (i+1, j, k)
