@@ -146,8 +146,18 @@ struct LdForce {
         vld<T, V>(psi, q, a);
         vld<T, V>(sp2, q, b);
         vld<T, V>(g, q, c);
+        if constexpr (V == 2) {
+            // the two points as one pair (lane-wise packed arithmetic)
+            const cpx<T> A{a[0], a[1]};
+            const cpx<T> p2 = pmul(A, A), p3 = pmul(p2, A);
+            const cpx<T> nl = pfma(cpx<T>{-gamma, -gamma}, pmul(p3, p2), pmul(cpx<T>{beta, beta}, p3));
+            const cpx<T> r = pmul(csub(cpx<T>{b[0], b[1]}, nl), cpx<T>{c[0], c[1]});
+            out[0] = r.x;
+            out[1] = r.y;
+        } else {
 #pragma unroll
-        for (int u = 0; u < V; u++) out[u] = (b[u] - nl3(a[u], beta, gamma)) * c[u];
+            for (int u = 0; u < V; u++) out[u] = (b[u] - nl3(a[u], beta, gamma)) * c[u];
+        }
     }
 };
 
